@@ -1,0 +1,106 @@
+// Device helpers shared by the kernel files (sm_100a, 32-lane warps).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace gcu {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFullMask = 0xFFFFFFFFu;
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_min(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        T w = __shfl_xor_sync(kFullMask, v, o);
+        v = w < v ? w : v;
+    }
+    return v;
+}
+
+// Inclusive warp scan.
+template <typename T>
+__device__ __forceinline__ T warp_inclusive_scan(T v) {
+    const unsigned lane = lane_id();
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T w = __shfl_up_sync(kFullMask, v, o);
+        if (lane >= static_cast<unsigned>(o)) v += w;
+    }
+    return v;
+}
+
+// Block-wide sum; every thread gets the result. `scratch` holds >= 32 values.
+template <typename T>
+__device__ __forceinline__ T block_sum(T v, T* scratch) {
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    const unsigned nwarps = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    T r = (threadIdx.x < nwarps) ? scratch[threadIdx.x] : T(0);
+    if (warp == 0) r = warp_sum(r);
+    if (threadIdx.x == 0) scratch[0] = r;
+    __syncthreads();
+    r = scratch[0];
+    __syncthreads();
+    return r;
+}
+
+// Streaming load that does not allocate in L1 (data read once).
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ uint4 ld_stream4(const uint4* p) {
+    uint4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+
+// First index in [lo, hi) with a[idx] >= val.
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t lo, uint32_t hi, uint32_t val) {
+    while (lo < hi) {
+        uint32_t mid = lo + ((hi - lo) >> 1);
+        if (a[mid] < val)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Largest row r in [0, n) with offsets[r] <= pos (offsets non-decreasing,
+// offsets[0] == 0 <= pos).
+__device__ __forceinline__ uint32_t row_of_entry(const uint32_t* offsets, uint32_t n, uint32_t pos) {
+    uint32_t lo = 0, hi = n;  // answer in [lo, hi)
+    while (hi - lo > 1) {
+        uint32_t mid = lo + ((hi - lo) >> 1);
+        if (offsets[mid] <= pos)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__host__ __device__ __forceinline__ uint64_t min_u64(uint64_t a, uint64_t b) { return a < b ? a : b; }
+
+__host__ __device__ __forceinline__ uint64_t ceil_div_u64(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+}  // namespace gcu

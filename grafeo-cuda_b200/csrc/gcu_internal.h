@@ -1,0 +1,221 @@
+// Internal declarations shared by the host runtime and the kernel files.
+//
+// Layout of a graph in HBM (one allocation each, 256-byte aligned, padded to a
+// multiple of 16 bytes plus 16 so that 16-byte vector and bulk loads of the
+// last partial chunk stay inside the allocation):
+//   offsets  u32[V + 1]   CSR row pointers   (GpuGraph::offsets, gpu_graph.rs:17)
+//   targets  u32[E]       sorted neighbours  (GpuGraph::targets, gpu_graph.rs:19)
+// Derived per-algorithm state (PageRank tile plan, BFS work buffers, ...) is
+// built lazily on first use and cached on the graph, like the reference caches
+// its kernel modules per context (module_cache.rs:23-87).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/grafeo_cuda.h"
+
+namespace gcu {
+
+// ---------------------------------------------------------------- errors
+
+// Error value carried through the host code; converted to gcu_status plus the
+// thread-local message at the C boundary.
+struct Error {
+    gcu_status status = GCU_OK;
+    std::string message;
+    bool ok() const { return status == GCU_OK; }
+};
+
+Error ok();
+Error no_device();
+Error driver_error(cudaError_t e, const char* what);
+Error out_of_memory(size_t required, size_t available);
+Error kernel_error(const std::string& msg);
+Error export_error(const std::string& msg);
+Error invalid_csr(const std::string& msg);
+
+// Records `e` as this thread's last error and returns its status.
+gcu_status fail(const Error& e);
+gcu_status succeed();
+
+#define GCU_TRY(expr)                       \
+    do {                                    \
+        ::gcu::Error _e = (expr);           \
+        if (!_e.ok()) return _e;            \
+    } while (0)
+
+#define GCU_CUDA(call, what)                                          \
+    do {                                                              \
+        cudaError_t _c = (call);                                      \
+        if (_c != cudaSuccess) return ::gcu::driver_error(_c, what);  \
+    } while (0)
+
+// ---------------------------------------------------------------- timing
+
+class WallTimer {
+  public:
+    WallTimer() : t0_(std::chrono::steady_clock::now()) {}
+    double seconds() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0_).count();
+    }
+
+  private:
+    std::chrono::steady_clock::time_point t0_;
+};
+
+// ---------------------------------------------------------------- device
+
+struct KernelStat {
+    uint64_t launches = 0;
+    double total_ms = 0.0;
+};
+
+struct DeviceImpl {
+    int ordinal = 0;
+    std::string name;
+    uint64_t total_memory = 0;
+    int sm_count = 0;
+    int l2_bytes = 0;
+    int max_smem_optin = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t timer_start = nullptr;
+    cudaEvent_t timer_stop = nullptr;
+
+    std::atomic<uint64_t> launches{0};
+    bool kernel_timing = false;
+    std::mutex stats_mu;
+    std::map<std::string, KernelStat> stats;
+    struct Pending {
+        const char* name;
+        cudaEvent_t start, stop;
+    };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> event_pool;
+
+    ~DeviceImpl();
+
+    // Makes this device current on the calling thread.
+    Error activate() const;
+    // Synchronizes the stream and folds pending per-kernel timings into stats.
+    Error sync();
+    // Called around each kernel launch by GCU_LAUNCH.
+    void before_launch(const char* name, cudaEvent_t* start);
+    void after_launch(const char* name, cudaEvent_t start);
+    void collect_pending();
+};
+
+// Stream-ordered device allocation that reports OutOfMemory with the
+// reference's required/available fields (error.rs:18-26).
+Error device_alloc(DeviceImpl& dev, void** ptr, size_t bytes);
+void device_free(DeviceImpl& dev, void* ptr);
+
+// Owning device buffer, freed on the device stream.
+template <typename T>
+struct DeviceBuffer {
+    DeviceImpl* dev = nullptr;
+    T* ptr = nullptr;
+    size_t count = 0;
+    DeviceBuffer() = default;
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept { *this = std::move(o); }
+    DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+        reset();
+        dev = o.dev; ptr = o.ptr; count = o.count;
+        o.ptr = nullptr; o.count = 0;
+        return *this;
+    }
+    ~DeviceBuffer() { reset(); }
+    Error allocate(DeviceImpl& d, size_t n) {
+        reset();
+        dev = &d;
+        count = n;
+        // Pad so that 16-byte vector loads of the tail stay in bounds.
+        size_t bytes = ((n * sizeof(T) + 15) / 16) * 16 + 16;
+        return device_alloc(d, reinterpret_cast<void**>(&ptr), bytes);
+    }
+    void reset() {
+        if (ptr && dev) device_free(*dev, ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+};
+
+// ---------------------------------------------------------------- graph
+
+struct PageRankPlan;
+struct BfsWork;
+
+struct GraphImpl {
+    std::shared_ptr<DeviceImpl> dev;
+    uint32_t num_nodes = 0;
+    uint32_t num_edges = 0;
+    DeviceBuffer<uint32_t> offsets;
+    DeviceBuffer<uint32_t> targets;
+    std::mutex mu;  // guards the lazily built caches below
+    PageRankPlan* pr_plan = nullptr;  // owned; freed by destroy_pagerank_plan
+    BfsWork* bfs_work = nullptr;      // owned; freed by destroy_bfs_work
+    ~GraphImpl();
+};
+
+// Host CSR arrays (CsrArrays, csr_export.rs:16-30).
+struct HostCsr {
+    std::vector<uint32_t> offsets;
+    std::vector<uint32_t> targets;
+    uint32_t num_nodes = 0;
+};
+
+// ---------------------------------------------------------------- host CSR
+
+Error validate_csr_host(const uint32_t* offsets, size_t n_offsets, const uint32_t* targets,
+                        size_t n_targets);
+// Exact validate_csr message for the first violation at or after `node`,
+// checking only that node (used after the device scan found it).
+std::string describe_node_violation(uint32_t node, uint32_t start, uint32_t end,
+                                    const uint32_t* list, size_t list_len, uint32_t num_nodes);
+
+// ---------------------------------------------------------------- kernels (host wrappers)
+
+// Finds the first node that breaks a CSR rule on the device; UINT32_MAX if none.
+Error validate_csr_device(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets,
+                          uint32_t num_nodes, uint32_t num_edges, uint32_t* first_bad_node);
+
+Error triangle_count(GraphImpl& g, bool oriented, uint64_t* total);
+Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reachable,
+          int32_t* max_depth);
+Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float tolerance,
+               float* host_ranks, uint32_t* iterations, bool* converged);
+Error k_truss(GraphImpl& g, uint32_t k, std::vector<uint32_t>* edges, uint32_t* iterations);
+
+// Exclusive scan of u32 counts into u32 offsets (out has n + 1 entries);
+// returns the total through the device (out[n]).
+Error exclusive_scan_u32(DeviceImpl& dev, const uint32_t* d_in, uint32_t* d_out, uint64_t n);
+
+void destroy_pagerank_plan(PageRankPlan* p);
+void destroy_bfs_work(BfsWork* w);
+
+}  // namespace gcu
+
+// Launch helper: counts the launch, brackets it with events when per-kernel
+// timing is on, and turns a launch failure into CudaError::Kernel.
+#define GCU_LAUNCH(devref, name, kernel, grid, block, smem, ...)                           \
+    do {                                                                                   \
+        cudaEvent_t _ev = nullptr;                                                         \
+        (devref).before_launch(name, &_ev);                                                \
+        kernel<<<(grid), (block), (smem), (devref).stream>>>(__VA_ARGS__);                 \
+        cudaError_t _le = cudaGetLastError();                                              \
+        (devref).after_launch(name, _ev);                                                  \
+        if (_le != cudaSuccess)                                                            \
+            return ::gcu::kernel_error(std::string(name) + " launch failed: " +            \
+                                       cudaGetErrorString(_le));                           \
+    } while (0)

@@ -1,0 +1,484 @@
+// Host runtime: errors, devices, graphs, timing, and the C ABI entry points
+// for them and for the algorithms.
+//
+// Mirrors crates/grafeo-cuda-core/src/{error.rs,device.rs,gpu_graph.rs} and the
+// PyO3-facing algorithm calls in crates/grafeo-cuda-algos/src/*.rs. Every call
+// runs on the device's own stream and synchronizes before returning, like the
+// reference's default-stream calls (device.rs:38).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <sstream>
+
+#include "gcu_internal.h"
+
+namespace gcu {
+
+// ---------------------------------------------------------------- errors
+
+static thread_local std::string t_last_error;
+
+Error ok() { return Error{}; }
+Error no_device() { return Error{GCU_ERR_NO_DEVICE, "no CUDA device found"}; }
+Error driver_error(cudaError_t e, const char* what) {
+    std::string msg = "CUDA driver error: ";
+    if (what && *what) {
+        msg += what;
+        msg += ": ";
+    }
+    msg += cudaGetErrorName(e);
+    msg += " (";
+    msg += cudaGetErrorString(e);
+    msg += ")";
+    return Error{GCU_ERR_DRIVER, msg};
+}
+Error out_of_memory(size_t required, size_t available) {
+    return Error{GCU_ERR_OUT_OF_MEMORY, "graph too large for GPU memory: " +
+                                            std::to_string(required) + " bytes required, " +
+                                            std::to_string(available) + " bytes available"};
+}
+Error kernel_error(const std::string& msg) { return Error{GCU_ERR_KERNEL, "kernel error: " + msg}; }
+Error export_error(const std::string& msg) {
+    return Error{GCU_ERR_EXPORT, "CSR export failed: " + msg};
+}
+Error invalid_csr(const std::string& msg) { return Error{GCU_ERR_INVALID_CSR, "invalid CSR: " + msg}; }
+
+gcu_status fail(const Error& e) {
+    t_last_error = e.message;
+    return e.status;
+}
+gcu_status succeed() {
+    t_last_error.clear();
+    return GCU_OK;
+}
+
+// ---------------------------------------------------------------- device
+
+DeviceImpl::~DeviceImpl() {
+    cudaSetDevice(ordinal);
+    if (stream) cudaStreamSynchronize(stream);
+    collect_pending();
+    for (auto e : event_pool) cudaEventDestroy(e);
+    if (timer_start) cudaEventDestroy(timer_start);
+    if (timer_stop) cudaEventDestroy(timer_stop);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+Error DeviceImpl::activate() const {
+    GCU_CUDA(cudaSetDevice(ordinal), "cudaSetDevice");
+    return ok();
+}
+
+Error DeviceImpl::sync() {
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return kernel_error(std::string("synchronize failed: ") + cudaGetErrorString(e));
+    collect_pending();
+    return ok();
+}
+
+void DeviceImpl::before_launch(const char* name, cudaEvent_t* start) {
+    (void)name;
+    launches.fetch_add(1, std::memory_order_relaxed);
+    *start = nullptr;
+    if (!kernel_timing) return;
+    cudaEvent_t e;
+    if (!event_pool.empty()) {
+        e = event_pool.back();
+        event_pool.pop_back();
+    } else if (cudaEventCreate(&e) != cudaSuccess) {
+        return;
+    }
+    cudaEventRecord(e, stream);
+    *start = e;
+}
+
+void DeviceImpl::after_launch(const char* name, cudaEvent_t start) {
+    if (!kernel_timing || start == nullptr) return;
+    cudaEvent_t e;
+    if (!event_pool.empty()) {
+        e = event_pool.back();
+        event_pool.pop_back();
+    } else if (cudaEventCreate(&e) != cudaSuccess) {
+        event_pool.push_back(start);
+        return;
+    }
+    cudaEventRecord(e, stream);
+    pending.push_back(Pending{name, start, e});
+    // Bound the number of outstanding events.
+    if (pending.size() > 4096) {
+        cudaStreamSynchronize(stream);
+        collect_pending();
+    }
+}
+
+void DeviceImpl::collect_pending() {
+    if (pending.empty()) return;
+    std::lock_guard<std::mutex> lock(stats_mu);
+    for (auto& p : pending) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(p.stop) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
+            KernelStat& s = stats[p.name];
+            s.launches += 1;
+            s.total_ms += ms;
+        }
+        event_pool.push_back(p.start);
+        event_pool.push_back(p.stop);
+    }
+    pending.clear();
+}
+
+Error device_alloc(DeviceImpl& dev, void** ptr, size_t bytes) {
+    *ptr = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMallocAsync(ptr, bytes, dev.stream);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        *ptr = nullptr;
+        return out_of_memory(bytes, free_b);
+    }
+    if (e != cudaSuccess) return driver_error(e, "cudaMallocAsync");
+    return ok();
+}
+
+void device_free(DeviceImpl& dev, void* ptr) {
+    if (ptr) cudaFreeAsync(ptr, dev.stream);
+}
+
+GraphImpl::~GraphImpl() {
+    if (dev) {
+        dev->activate();
+        destroy_pagerank_plan(pr_plan);
+        destroy_bfs_work(bfs_work);
+        pr_plan = nullptr;
+        bfs_work = nullptr;
+        offsets.reset();
+        targets.reset();
+        cudaStreamSynchronize(dev->stream);
+    }
+}
+
+static Error create_device(int ordinal, std::shared_ptr<DeviceImpl>* out) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || (e == cudaSuccess && count == 0)) {
+        cudaGetLastError();
+        return no_device();
+    }
+    if (e != cudaSuccess) return driver_error(e, "cudaGetDeviceCount");
+    if (ordinal < 0 || ordinal >= count) {
+        return driver_error(cudaErrorInvalidDevice, ("device ordinal " + std::to_string(ordinal)).c_str());
+    }
+    auto dev = std::make_shared<DeviceImpl>();
+    dev->ordinal = ordinal;
+    GCU_CUDA(cudaSetDevice(ordinal), "cudaSetDevice");
+    cudaDeviceProp prop;
+    GCU_CUDA(cudaGetDeviceProperties(&prop, ordinal), "cudaGetDeviceProperties");
+    dev->name = prop.name;
+    dev->total_memory = prop.totalGlobalMem;
+    dev->sm_count = prop.multiProcessorCount;
+    dev->l2_bytes = prop.l2CacheSize;
+    dev->max_smem_optin = static_cast<int>(prop.sharedMemPerBlockOptin);
+    GCU_CUDA(cudaStreamCreateWithFlags(&dev->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    GCU_CUDA(cudaEventCreate(&dev->timer_start), "cudaEventCreate");
+    GCU_CUDA(cudaEventCreate(&dev->timer_stop), "cudaEventCreate");
+    // Keep freed stream-ordered allocations cached in the pool, so repeated
+    // algorithm calls do not return memory to the driver between calls.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ordinal) == cudaSuccess) {
+        uint64_t threshold = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    *out = dev;
+    return ok();
+}
+
+}  // namespace gcu
+
+using namespace gcu;
+
+struct gcu_device {
+    std::shared_ptr<DeviceImpl> impl;
+};
+struct gcu_graph {
+    std::unique_ptr<GraphImpl> impl;
+};
+struct gcu_edge_list {
+    std::vector<uint32_t> data;
+};
+
+// ---------------------------------------------------------------- C ABI
+
+extern "C" {
+
+GCU_API const char* gcu_last_error(void) { return t_last_error.c_str(); }
+GCU_API const char* gcu_version(void) { return "0.3.0+b200"; }
+
+GCU_API int gcu_device_count(void) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return count;
+}
+
+GCU_API gcu_status gcu_device_create(int ordinal, gcu_device** out) {
+    if (!out) return fail(kernel_error("gcu_device_create: out is NULL"));
+    *out = nullptr;
+    std::shared_ptr<DeviceImpl> impl;
+    Error e = create_device(ordinal, &impl);
+    if (!e.ok()) return fail(e);
+    *out = new gcu_device{impl};
+    return succeed();
+}
+
+GCU_API void gcu_device_destroy(gcu_device* dev) { delete dev; }
+GCU_API const char* gcu_device_name(const gcu_device* dev) { return dev ? dev->impl->name.c_str() : ""; }
+GCU_API int gcu_device_ordinal(const gcu_device* dev) { return dev ? dev->impl->ordinal : -1; }
+GCU_API uint64_t gcu_device_total_memory(const gcu_device* dev) { return dev ? dev->impl->total_memory : 0; }
+GCU_API int gcu_device_sm_count(const gcu_device* dev) { return dev ? dev->impl->sm_count : 0; }
+GCU_API void* gcu_device_stream(gcu_device* dev) { return dev ? static_cast<void*>(dev->impl->stream) : nullptr; }
+
+GCU_API gcu_status gcu_device_synchronize(gcu_device* dev) {
+    if (!dev) return fail(kernel_error("device is NULL"));
+    Error e = dev->impl->activate();
+    if (e.ok()) e = dev->impl->sync();
+    return e.ok() ? succeed() : fail(e);
+}
+
+GCU_API gcu_status gcu_device_timer_start(gcu_device* dev) {
+    if (!dev) return fail(kernel_error("device is NULL"));
+    DeviceImpl& d = *dev->impl;
+    Error e = d.activate();
+    if (!e.ok()) return fail(e);
+    cudaError_t c = cudaEventRecord(d.timer_start, d.stream);
+    if (c != cudaSuccess) return fail(driver_error(c, "cudaEventRecord"));
+    return succeed();
+}
+
+GCU_API gcu_status gcu_device_timer_stop(gcu_device* dev, float* ms) {
+    if (!dev) return fail(kernel_error("device is NULL"));
+    DeviceImpl& d = *dev->impl;
+    Error e = d.activate();
+    if (!e.ok()) return fail(e);
+    cudaError_t c = cudaEventRecord(d.timer_stop, d.stream);
+    if (c == cudaSuccess) c = cudaEventSynchronize(d.timer_stop);
+    float t = 0.f;
+    if (c == cudaSuccess) c = cudaEventElapsedTime(&t, d.timer_start, d.timer_stop);
+    if (c != cudaSuccess) return fail(driver_error(c, "event timing"));
+    if (ms) *ms = t;
+    return succeed();
+}
+
+GCU_API uint64_t gcu_device_launch_count(const gcu_device* dev) {
+    return dev ? dev->impl->launches.load() : 0;
+}
+
+GCU_API void gcu_device_set_kernel_timing(gcu_device* dev, int on) {
+    if (!dev) return;
+    dev->impl->activate();
+    cudaStreamSynchronize(dev->impl->stream);
+    dev->impl->collect_pending();
+    dev->impl->kernel_timing = on != 0;
+}
+
+GCU_API size_t gcu_device_kernel_stats(gcu_device* dev, char* buf, size_t buflen) {
+    if (!dev) return 0;
+    DeviceImpl& d = *dev->impl;
+    d.activate();
+    cudaStreamSynchronize(d.stream);
+    d.collect_pending();
+    std::ostringstream os;
+    os.precision(9);
+    os << "{";
+    {
+        std::lock_guard<std::mutex> lock(d.stats_mu);
+        bool first = true;
+        for (auto& kv : d.stats) {
+            if (!first) os << ", ";
+            first = false;
+            os << "\"" << kv.first << "\": [" << kv.second.launches << ", " << kv.second.total_ms << "]";
+        }
+    }
+    os << "}";
+    std::string s = os.str();
+    if (buf && buflen) {
+        size_t n = std::min(buflen - 1, s.size());
+        std::memcpy(buf, s.data(), n);
+        buf[n] = 0;
+    }
+    return s.size() + 1;
+}
+
+GCU_API void gcu_device_reset_stats(gcu_device* dev) {
+    if (!dev) return;
+    DeviceImpl& d = *dev->impl;
+    d.activate();
+    cudaStreamSynchronize(d.stream);
+    d.collect_pending();
+    std::lock_guard<std::mutex> lock(d.stats_mu);
+    d.stats.clear();
+    d.launches.store(0);
+}
+
+GCU_API gcu_status gcu_graph_from_csr(gcu_device* dev, const uint32_t* offsets, size_t n_offsets,
+                                      const uint32_t* targets, size_t n_targets, gcu_graph** out) {
+    if (!out) return fail(kernel_error("gcu_graph_from_csr: out is NULL"));
+    *out = nullptr;
+    if (!dev) return fail(kernel_error("device is NULL"));
+    // Shape checks need only a few host reads; the per-entry rules run on the
+    // device after the copy (csr_export.rs:71-96 for the order of the checks).
+    if (n_offsets == 0) {
+        return fail(invalid_csr("offsets must have num_nodes + 1 entries, got an empty array"));
+    }
+    if (n_offsets > 0xFFFFFFFFull || n_targets > 0xFFFFFFFFull) {
+        return fail(invalid_csr("graph too large for u32 indices: " + std::to_string(n_offsets) +
+                                " offsets, " + std::to_string(n_targets) + " targets"));
+    }
+    if (!offsets || (n_targets > 0 && !targets)) return fail(kernel_error("CSR pointer is NULL"));
+    if (offsets[0] != 0) {
+        return fail(invalid_csr("offsets[0] must be 0, got " + std::to_string(offsets[0])));
+    }
+    const size_t num_nodes = n_offsets - 1;
+    if (static_cast<size_t>(offsets[num_nodes]) != n_targets) {
+        return fail(invalid_csr("offsets[" + std::to_string(num_nodes) + "] is " +
+                                std::to_string(offsets[num_nodes]) + " but targets has " +
+                                std::to_string(n_targets) + " entries"));
+    }
+
+    WallTimer wall;
+    (void)wall;
+    auto g = std::make_unique<GraphImpl>();
+    g->dev = dev->impl;
+    DeviceImpl& d = *g->dev;
+    Error e = d.activate();
+    if (!e.ok()) return fail(e);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        size_t required = n_offsets * 4 + n_targets * 4;
+        if (required > free_b) return fail(out_of_memory(required, free_b));
+    }
+    g->num_nodes = static_cast<uint32_t>(num_nodes);
+    g->num_edges = static_cast<uint32_t>(n_targets);
+    e = g->offsets.allocate(d, n_offsets);
+    if (e.ok()) e = g->targets.allocate(d, n_targets);
+    if (!e.ok()) return fail(e);
+    cudaError_t c = cudaMemcpyAsync(g->offsets.ptr, offsets, n_offsets * 4, cudaMemcpyHostToDevice, d.stream);
+    if (c == cudaSuccess && n_targets)
+        c = cudaMemcpyAsync(g->targets.ptr, targets, n_targets * 4, cudaMemcpyHostToDevice, d.stream);
+    if (c != cudaSuccess) return fail(driver_error(c, "copy CSR to device"));
+
+    uint32_t bad = UINT32_MAX;
+    e = validate_csr_device(d, g->offsets.ptr, g->targets.ptr, g->num_nodes, g->num_edges, &bad);
+    if (!e.ok()) return fail(e);
+    if (bad != UINT32_MAX) {
+        // Reproduce the exact reference message for that node on the host.
+        uint32_t start = offsets[bad], end = offsets[bad + 1];
+        size_t lo = std::min<size_t>(start, n_targets), hi = std::min<size_t>(std::max(start, end), n_targets);
+        std::string msg = describe_node_violation(bad, start, end, targets + lo, hi - lo, g->num_nodes);
+        return fail(invalid_csr(msg));
+    }
+    *out = new gcu_graph{std::move(g)};
+    return succeed();
+}
+
+GCU_API uint32_t gcu_graph_num_nodes(const gcu_graph* g) { return g ? g->impl->num_nodes : 0; }
+GCU_API uint32_t gcu_graph_num_edges(const gcu_graph* g) { return g ? g->impl->num_edges : 0; }
+GCU_API void gcu_graph_destroy(gcu_graph* g) { delete g; }
+
+GCU_API gcu_status gcu_triangle_count(gcu_graph* g, uint64_t* total, double* seconds) {
+    WallTimer wall;
+    if (!g) return fail(kernel_error("graph is NULL"));
+    std::lock_guard<std::mutex> lock(g->impl->mu);
+    Error e = g->impl->dev->activate();
+    uint64_t t = 0;
+    if (e.ok()) e = triangle_count(*g->impl, false, &t);
+    if (!e.ok()) return fail(e);
+    if (total) *total = t;
+    if (seconds) *seconds = wall.seconds();
+    return succeed();
+}
+
+GCU_API gcu_status gcu_triangle_count_oriented(gcu_graph* g, uint64_t* total, double* seconds) {
+    WallTimer wall;
+    if (!g) return fail(kernel_error("graph is NULL"));
+    std::lock_guard<std::mutex> lock(g->impl->mu);
+    Error e = g->impl->dev->activate();
+    uint64_t t = 0;
+    if (e.ok()) e = triangle_count(*g->impl, true, &t);
+    if (!e.ok()) return fail(e);
+    if (total) *total = t;
+    if (seconds) *seconds = wall.seconds();
+    return succeed();
+}
+
+GCU_API gcu_status gcu_bfs(gcu_graph* g, uint32_t source, int32_t* distances, uint32_t* reachable,
+                           int32_t* max_depth, double* seconds) {
+    WallTimer wall;
+    if (!g) return fail(kernel_error("graph is NULL"));
+    GraphImpl& gi = *g->impl;
+    // bfs.rs:46-51
+    if (source >= gi.num_nodes) {
+        return fail(kernel_error("source node " + std::to_string(source) +
+                                 " out of range (num_nodes = " + std::to_string(gi.num_nodes) + ")"));
+    }
+    std::lock_guard<std::mutex> lock(gi.mu);
+    Error e = gi.dev->activate();
+    uint32_t r = 0;
+    int32_t depth = 0;
+    if (e.ok()) e = bfs(gi, source, distances, &r, &depth);
+    if (!e.ok()) return fail(e);
+    if (reachable) *reachable = r;
+    if (max_depth) *max_depth = depth;
+    if (seconds) *seconds = wall.seconds();
+    return succeed();
+}
+
+GCU_API gcu_status gcu_pagerank(gcu_graph* g, float damping, uint32_t max_iterations, float tolerance,
+                                float* ranks, uint32_t* iterations, int* converged, double* seconds) {
+    WallTimer wall;
+    if (!g) return fail(kernel_error("graph is NULL"));
+    GraphImpl& gi = *g->impl;
+    std::lock_guard<std::mutex> lock(gi.mu);
+    Error e = gi.dev->activate();
+    uint32_t it = 0;
+    bool conv = false;
+    if (e.ok()) e = pagerank(gi, damping, max_iterations, tolerance, ranks, &it, &conv);
+    if (!e.ok()) return fail(e);
+    if (iterations) *iterations = it;
+    if (converged) *converged = conv ? 1 : 0;
+    if (seconds) *seconds = wall.seconds();
+    return succeed();
+}
+
+GCU_API gcu_status gcu_k_truss(gcu_graph* g, uint32_t k, gcu_edge_list** edges, uint32_t* iterations,
+                               double* seconds) {
+    WallTimer wall;
+    if (edges) *edges = nullptr;
+    if (!g) return fail(kernel_error("graph is NULL"));
+    // k_truss.rs:43-47
+    if (k < 3) return fail(kernel_error("k must be >= 3 for k-truss decomposition"));
+    GraphImpl& gi = *g->impl;
+    std::lock_guard<std::mutex> lock(gi.mu);
+    Error e = gi.dev->activate();
+    auto list = std::make_unique<gcu_edge_list>();
+    uint32_t it = 0;
+    if (e.ok()) e = k_truss(gi, k, &list->data, &it);
+    if (!e.ok()) return fail(e);
+    if (iterations) *iterations = it;
+    if (seconds) *seconds = wall.seconds();
+    if (edges) *edges = list.release();
+    return succeed();
+}
+
+GCU_API size_t gcu_edge_list_len(const gcu_edge_list* list) { return list ? list->data.size() / 2 : 0; }
+GCU_API const uint32_t* gcu_edge_list_data(const gcu_edge_list* list) {
+    return list && !list->data.empty() ? list->data.data() : nullptr;
+}
+GCU_API void gcu_edge_list_free(gcu_edge_list* list) { delete list; }
+
+}  // extern "C"

@@ -1,0 +1,108 @@
+// Device-wide exclusive scan of u32 counts into CSR-style offsets.
+//
+// Replaces the reference's single-thread `prefix_sum_kernel`
+// (crates/grafeo-cuda-algos/kernels/triangle_counting.cu:223-237), a serial
+// O(V) loop on one GPU thread. Three passes: per-tile sums, a scan of the tile
+// sums in one block, then the per-tile scan with its carry-in. Each tile is
+// 1024 threads x 8 items; the input is read twice and the output written once.
+#include "device_common.cuh"
+#include "gcu_internal.h"
+
+namespace gcu {
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__global__ void __launch_bounds__(kScanThreads) scan_tile_sums_kernel(const uint32_t* __restrict__ in, uint64_t n,
+                                                                     uint32_t* __restrict__ tile_sums) {
+    __shared__ uint32_t scratch[32];
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile;
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        uint64_t i = base + static_cast<uint64_t>(k) * kScanThreads + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    s = block_sum(s, scratch);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = s;
+}
+
+// Exclusive scan of the tile sums in place; writes the grand total to *total.
+__global__ void __launch_bounds__(kScanThreads) scan_tile_prefix_kernel(uint32_t* __restrict__ tile_sums,
+                                                                       uint64_t num_tiles, uint32_t* __restrict__ total) {
+    __shared__ uint32_t warp_tot[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    for (uint64_t base = 0; base < num_tiles; base += kScanThreads) {
+        uint64_t i = base + threadIdx.x;
+        uint32_t v = i < num_tiles ? tile_sums[i] : 0;
+        uint32_t inc = warp_inclusive_scan(v);
+        if (lane == 31) warp_tot[warp] = inc;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = warp_tot[lane];
+            uint32_t winc = warp_inclusive_scan(w);
+            warp_tot[lane] = winc - w;
+        }
+        __syncthreads();
+        uint32_t excl = carry + warp_tot[warp] + inc - v;
+        if (i < num_tiles) tile_sums[i] = excl;
+        __syncthreads();
+        if (threadIdx.x == kScanThreads - 1) carry = excl + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const uint32_t* __restrict__ in, uint64_t n,
+                                                                 const uint32_t* __restrict__ tile_prefix,
+                                                                 uint32_t* __restrict__ out) {
+    __shared__ uint32_t warp_tot[32];
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile;
+    // Thread t owns items base + t*8 .. base + t*8 + 7 (a blocked layout).
+    uint32_t v[kScanItems];
+    uint32_t local = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        uint64_t i = base + static_cast<uint64_t>(threadIdx.x) * kScanItems + k;
+        v[k] = i < n ? in[i] : 0;
+        local += v[k];
+    }
+    uint32_t inc = warp_inclusive_scan(local);
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = warp_tot[lane];
+        warp_tot[lane] = warp_inclusive_scan(w) - w;
+    }
+    __syncthreads();
+    uint32_t run = tile_prefix[blockIdx.x] + warp_tot[warp] + inc - local;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        uint64_t i = base + static_cast<uint64_t>(threadIdx.x) * kScanItems + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+    }
+}
+
+Error exclusive_scan_u32(DeviceImpl& dev, const uint32_t* d_in, uint32_t* d_out, uint64_t n) {
+    if (n == 0) {
+        GCU_CUDA(cudaMemsetAsync(d_out, 0, sizeof(uint32_t), dev.stream), "memset");
+        return ok();
+    }
+    const uint64_t tiles = ceil_div_u64(n, kScanTile);
+    DeviceBuffer<uint32_t> sums;
+    GCU_TRY(sums.allocate(dev, tiles));
+    GCU_LAUNCH(dev, "scan_tile_sums", scan_tile_sums_kernel, static_cast<unsigned>(tiles), kScanThreads, 0, d_in, n,
+               sums.ptr);
+    GCU_LAUNCH(dev, "scan_tile_prefix", scan_tile_prefix_kernel, 1, kScanThreads, 0, sums.ptr, tiles, d_out + n);
+    GCU_LAUNCH(dev, "scan_tiles", scan_tiles_kernel, static_cast<unsigned>(tiles), kScanThreads, 0, d_in, n, sums.ptr,
+               d_out);
+    return ok();
+}
+
+}  // namespace gcu

@@ -1,0 +1,178 @@
+/*
+ * grafeo_cuda.h — C ABI of the B200 (sm_100a) graph hot paths.
+ *
+ * This is the drop-in boundary for the four algorithm paths of grafeo-cuda
+ * (triangle counting, BFS, PageRank, k-truss). Every entry point takes plain
+ * pointers and sizes; no CUDA or torch types appear in the signatures. Each
+ * declaration names the reference interface it replaces (file:line inside the
+ * grafeo-cuda project). The reference's host side is Rust; a Rust `-sys` crate,
+ * the Python module and the C++ tools all bind to these symbols.
+ *
+ * Conventions
+ *  - Every fallible call returns a gcu_status. On failure the thread-local
+ *    message returned by gcu_last_error() holds the same text as the
+ *    reference's `CudaError` Display impl (crates/grafeo-cuda-core/src/error.rs:5-38).
+ *  - Calls are synchronous, like the reference's (each syncs its stream before
+ *    returning). Results are written into caller-owned host buffers unless a
+ *    function says otherwise.
+ *  - `seconds` out-parameters are host wall time around the whole call,
+ *    including allocation and result copies, as the reference's `time_seconds`
+ *    (e.g. crates/grafeo-cuda-algos/src/bfs.rs:43,121-123). They may be NULL.
+ */
+#ifndef GRAFEO_CUDA_H
+#define GRAFEO_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define GCU_API __attribute__((visibility("default")))
+#else
+#define GCU_API
+#endif
+
+/* ---- status / errors: crates/grafeo-cuda-core/src/error.rs:5-38 ---- */
+
+typedef enum gcu_status {
+    GCU_OK = 0,
+    GCU_ERR_NO_DEVICE = 1,     /* CudaError::NoDevice */
+    GCU_ERR_DRIVER = 2,        /* CudaError::Driver */
+    GCU_ERR_OUT_OF_MEMORY = 3, /* CudaError::OutOfMemory{required, available} */
+    GCU_ERR_KERNEL = 4,        /* CudaError::Kernel (also argument errors) */
+    GCU_ERR_EXPORT = 5,        /* CudaError::Export */
+    GCU_ERR_INVALID_CSR = 6    /* CudaError::InvalidCsr */
+} gcu_status;
+
+/* Message of the last failed call on this thread ("" if none). */
+GCU_API const char* gcu_last_error(void);
+/* Library version string, e.g. "0.3.0+b200". */
+GCU_API const char* gcu_version(void);
+/* Number of visible CUDA devices (0 when there is no driver or device). */
+GCU_API int gcu_device_count(void);
+
+/* ---- device: crates/grafeo-cuda-core/src/device.rs:9-66 ---- */
+
+typedef struct gcu_device gcu_device;
+
+/* GpuDevice::new(ordinal) (device.rs:30). Creates one stream for the device. */
+GCU_API gcu_status gcu_device_create(int ordinal, gcu_device** out);
+/* Drops this handle. Graphs created on it keep the device alive. */
+GCU_API void gcu_device_destroy(gcu_device* dev);
+/* DeviceProperties{name, ordinal, total_memory} (device.rs:9-17,54). */
+GCU_API const char* gcu_device_name(const gcu_device* dev);
+GCU_API int gcu_device_ordinal(const gcu_device* dev);
+GCU_API uint64_t gcu_device_total_memory(const gcu_device* dev);
+GCU_API int gcu_device_sm_count(const gcu_device* dev);
+/* GpuDevice::stream() (device.rs:64): the cudaStream_t every call runs on. */
+GCU_API void* gcu_device_stream(gcu_device* dev);
+GCU_API gcu_status gcu_device_synchronize(gcu_device* dev);
+
+/* Device-time measurement on the device stream (CUDA events), for benchmarks:
+ * start records an event, stop records a second one, synchronizes and
+ * returns the elapsed milliseconds. Replaces the reference's wall-clock
+ * best-of-N (crates/grafeo-cuda-algos/src/bin/gpu_bfs.rs:63-83). */
+GCU_API gcu_status gcu_device_timer_start(gcu_device* dev);
+GCU_API gcu_status gcu_device_timer_stop(gcu_device* dev, float* ms);
+/* Number of kernels this library has launched on the device. */
+GCU_API uint64_t gcu_device_launch_count(const gcu_device* dev);
+/* When on, every kernel launch is bracketed by CUDA events and its device time
+ * is accumulated per kernel name. */
+GCU_API void gcu_device_set_kernel_timing(gcu_device* dev, int on);
+/* Writes per-kernel statistics as JSON {"name": [launches, total_ms], ...}
+ * into buf (always NUL-terminated) and returns the full length needed. */
+GCU_API size_t gcu_device_kernel_stats(gcu_device* dev, char* buf, size_t buflen);
+GCU_API void gcu_device_reset_stats(gcu_device* dev);
+
+/* ---- host CSR arrays: crates/grafeo-cuda-core/src/csr_export.rs ---- */
+
+typedef struct gcu_csr gcu_csr; /* CsrArrays (csr_export.rs:16-30), host memory */
+
+/* validate_csr(offsets, targets) (csr_export.rs:71-120), on the host. */
+GCU_API gcu_status gcu_validate_csr(const uint32_t* offsets, size_t n_offsets,
+                                    const uint32_t* targets, size_t n_targets);
+/* from_edge_pairs(edges, num_nodes, symmetric) (csr_export.rs:202-239).
+ * pairs holds n_pairs (src, dst) pairs interleaved. */
+GCU_API gcu_status gcu_csr_from_edge_pairs(const uint32_t* pairs, size_t n_pairs,
+                                           uint32_t num_nodes, int symmetric,
+                                           gcu_csr** out);
+/* from_edge_pairs_oriented(edges, num_nodes) (csr_export.rs:299-350). */
+GCU_API gcu_status gcu_csr_from_edge_pairs_oriented(const uint32_t* pairs, size_t n_pairs,
+                                                    uint32_t num_nodes, gcu_csr** out);
+/* parse_tsv_to_edges(path) (csr_export.rs:246-287). *pairs is freed with
+ * gcu_free_pairs. A missing file is GCU_ERR_EXPORT. */
+GCU_API gcu_status gcu_parse_tsv_to_edges(const char* path, uint32_t** pairs,
+                                          size_t* n_pairs, uint32_t* num_nodes);
+GCU_API void gcu_free_pairs(uint32_t* pairs);
+/* Synthetic inputs standing in for Graph500/GraphChallenge files (which the
+ * reference loads through parse_tsv_to_edges): R-MAT and Erdos-Renyi, built
+ * symmetric without self-loops or duplicates, from a counter-based SplitMix64
+ * stream so the graph is the same for any thread count. */
+GCU_API gcu_status gcu_generate_rmat(uint32_t scale, uint32_t edge_factor, double a,
+                                     double b, double c, uint64_t seed, gcu_csr** out);
+GCU_API gcu_status gcu_generate_erdos_renyi(uint32_t num_nodes, uint64_t num_pairs,
+                                            uint64_t seed, gcu_csr** out);
+GCU_API uint32_t gcu_csr_num_nodes(const gcu_csr* csr);
+GCU_API uint64_t gcu_csr_num_edges(const gcu_csr* csr);
+GCU_API const uint32_t* gcu_csr_offsets(const gcu_csr* csr);
+GCU_API const uint32_t* gcu_csr_targets(const gcu_csr* csr);
+GCU_API void gcu_csr_free(gcu_csr* csr);
+
+/* ---- device graph: crates/grafeo-cuda-core/src/gpu_graph.rs:15-88 ---- */
+
+typedef struct gcu_graph gcu_graph;
+
+/* GpuGraph::from_csr_slices(offsets, targets, device) (gpu_graph.rs:66-88) and
+ * from_csr_arrays (gpu_graph.rs:46-60). Copies the arrays to the device and
+ * validates them there with the same rules and messages as validate_csr;
+ * an invalid CSR is GCU_ERR_INVALID_CSR and no graph is returned. */
+GCU_API gcu_status gcu_graph_from_csr(gcu_device* dev, const uint32_t* offsets,
+                                      size_t n_offsets, const uint32_t* targets,
+                                      size_t n_targets, gcu_graph** out);
+GCU_API uint32_t gcu_graph_num_nodes(const gcu_graph* g);
+GCU_API uint32_t gcu_graph_num_edges(const gcu_graph* g);
+GCU_API void gcu_graph_destroy(gcu_graph* g);
+
+/* ---- algorithms: crates/grafeo-cuda-algos/src ---- */
+
+/* triangle_counting::triangle_count (triangle_counting.rs:40-152): total
+ * triangles of the undirected simple graph in a symmetric CSR. */
+GCU_API gcu_status gcu_triangle_count(gcu_graph* g, uint64_t* total, double* seconds);
+/* triangle_counting::triangle_count_oriented (triangle_counting.rs:162-210):
+ * sum over CSR entries u->v of |N(u) ∩ N(v)|, for a degree-oriented CSR. */
+GCU_API gcu_status gcu_triangle_count_oriented(gcu_graph* g, uint64_t* total,
+                                               double* seconds);
+
+/* bfs::bfs(graph, source) (bfs.rs:42-131). distances (num_nodes i32, -1 =
+ * unreachable) may be NULL, in which case the distances stay on the device.
+ * A source >= num_nodes is GCU_ERR_KERNEL. */
+GCU_API gcu_status gcu_bfs(gcu_graph* g, uint32_t source, int32_t* distances,
+                           uint32_t* reachable, int32_t* max_depth, double* seconds);
+
+/* pagerank::pagerank(graph, damping, max_iterations, tolerance)
+ * (pagerank.rs:46-199). ranks (num_nodes f32) may be NULL, in which case the
+ * ranks stay on the device. Convergence: L1 change between iterations below
+ * tolerance (pagerank.rs:150-182). */
+GCU_API gcu_status gcu_pagerank(gcu_graph* g, float damping, uint32_t max_iterations,
+                                float tolerance, float* ranks, uint32_t* iterations,
+                                int* converged, double* seconds);
+
+typedef struct gcu_edge_list gcu_edge_list; /* Vec<(u32, u32)>, host memory */
+
+/* k_truss::k_truss(graph, k) (k_truss.rs:42-161). Edges (u, v) with u < v in
+ * CSR order. k < 3 is GCU_ERR_KERNEL. */
+GCU_API gcu_status gcu_k_truss(gcu_graph* g, uint32_t k, gcu_edge_list** edges,
+                               uint32_t* iterations, double* seconds);
+GCU_API size_t gcu_edge_list_len(const gcu_edge_list* list);
+/* 2 * len values: u0, v0, u1, v1, ... */
+GCU_API const uint32_t* gcu_edge_list_data(const gcu_edge_list* list);
+GCU_API void gcu_edge_list_free(gcu_edge_list* list);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAFEO_CUDA_H */

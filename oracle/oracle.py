@@ -1,0 +1,139 @@
+"""Oracle — TEST INFRASTRUCTURE ONLY (ctypes wrapper of liboracle.so).
+
+Loads the C restatement in oracle.c (building it with `make` when the shared
+library is missing). Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg import this module; the product never does. See oracle.h for
+what each function restates and how the oracle is pinned.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+u32p = C.POINTER(C.c_uint32)
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "oracle.c")
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+        subprocess.run(["make", "-B", "-C", HERE], check=True, capture_output=True)
+    return LIB_PATH
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = C.CDLL(LIB_PATH)
+    lib.orc_triangle_count.restype = C.c_uint64
+    lib.orc_triangle_count.argtypes = [u32p, u32p, C.c_uint32]
+    lib.orc_triangle_count_oriented.restype = C.c_uint64
+    lib.orc_triangle_count_oriented.argtypes = [u32p, u32p, C.c_uint32]
+    lib.orc_bfs.restype = None
+    lib.orc_bfs.argtypes = [u32p, u32p, C.c_uint32, C.c_uint32, C.POINTER(C.c_int32), u32p, C.POINTER(C.c_int32)]
+    lib.orc_pagerank.restype = None
+    lib.orc_pagerank.argtypes = [
+        u32p, u32p, C.c_uint32, u32p, C.c_double, C.c_uint32, C.c_double, C.c_int,
+        C.POINTER(C.c_double), u32p, C.POINTER(C.c_int),
+    ]
+    lib.orc_k_truss.restype = C.c_size_t
+    lib.orc_k_truss.argtypes = [u32p, u32p, C.c_uint32, C.c_uint32, u32p, u32p]
+    lib.orc_from_edge_pairs.restype = C.c_size_t
+    lib.orc_from_edge_pairs.argtypes = [u32p, C.c_size_t, C.c_uint32, C.c_int, u32p, u32p]
+    lib.orc_from_edge_pairs_oriented.restype = C.c_size_t
+    lib.orc_from_edge_pairs_oriented.argtypes = [u32p, C.c_size_t, C.c_uint32, u32p, u32p]
+    lib.orc_num_threads.restype = C.c_int
+    lib.orc_num_threads.argtypes = []
+    return lib
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = _load()
+    return _lib
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+
+
+def _p(a: np.ndarray, t=C.c_uint32):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
+
+
+def triangle_count(offsets, targets) -> int:
+    o, t = _u32(offsets), _u32(targets)
+    return int(lib().orc_triangle_count(_p(o), _p(t), len(o) - 1))
+
+
+def triangle_count_oriented(offsets, targets) -> int:
+    o, t = _u32(offsets), _u32(targets)
+    return int(lib().orc_triangle_count_oriented(_p(o), _p(t), len(o) - 1))
+
+
+def bfs(offsets, targets, source: int) -> dict:
+    o, t = _u32(offsets), _u32(targets)
+    n = len(o) - 1
+    dist = np.empty(max(n, 1), dtype=np.int32)
+    reach = C.c_uint32()
+    depth = C.c_int32()
+    lib().orc_bfs(_p(o), _p(t), n, int(source), _p(dist, C.c_int32), C.byref(reach), C.byref(depth))
+    return {"distances": dist[:n], "reachable": int(reach.value), "max_depth": int(depth.value)}
+
+
+def pagerank(offsets, targets, damping=0.85, max_iterations=100, tolerance=1e-6, rule="l1",
+             out_degree=None) -> dict:
+    """rule 'l1': the reference GPU stopping rule; 'max': Grafeo's."""
+    o, t = _u32(offsets), _u32(targets)
+    n = len(o) - 1
+    ranks = np.zeros(max(n, 1), dtype=np.float64)
+    it = C.c_uint32()
+    conv = C.c_int()
+    od = None if out_degree is None else _u32(out_degree)
+    lib().orc_pagerank(
+        _p(o), _p(t), n, None if od is None else _p(od), float(damping), int(max_iterations), float(tolerance),
+        0 if rule == "l1" else 1, _p(ranks, C.c_double), C.byref(it), C.byref(conv),
+    )
+    return {"ranks": ranks[:n], "iterations": int(it.value), "converged": bool(conv.value)}
+
+
+def k_truss(offsets, targets, k: int) -> dict:
+    o, t = _u32(offsets), _u32(targets)
+    n = len(o) - 1
+    out = np.zeros(max(2 * len(t), 2), dtype=np.uint32)
+    it = C.c_uint32()
+    m = int(lib().orc_k_truss(_p(o), _p(t), n, int(k), _p(out), C.byref(it)))
+    return {"edges": out[: 2 * m].reshape(m, 2), "iterations": int(it.value)}
+
+
+def from_edge_pairs(edges, num_nodes: int, symmetric: bool):
+    p = _u32(edges).reshape(-1)
+    offsets = np.zeros(num_nodes + 1, dtype=np.uint32)
+    targets = np.zeros(max(len(p), 1), dtype=np.uint32)
+    m = lib().orc_from_edge_pairs(_p(p), len(p) // 2, num_nodes, 1 if symmetric else 0, _p(offsets), _p(targets))
+    if m == C.c_size_t(-1).value:
+        raise ValueError("edge references a node >= num_nodes")
+    return offsets, targets[:m]
+
+
+def from_edge_pairs_oriented(edges, num_nodes: int):
+    p = _u32(edges).reshape(-1)
+    offsets = np.zeros(num_nodes + 1, dtype=np.uint32)
+    targets = np.zeros(max(len(p) // 2, 1), dtype=np.uint32)
+    m = lib().orc_from_edge_pairs_oriented(_p(p), len(p) // 2, num_nodes, _p(offsets), _p(targets))
+    if m == C.c_size_t(-1).value:
+        raise ValueError("edge references a node >= num_nodes")
+    return offsets, targets[:m]

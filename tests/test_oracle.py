@@ -1,0 +1,145 @@
+"""Pins the oracle before anything is compared with it (CPU only).
+
+The oracle (oracle/oracle.c) must reproduce the literal answers written in
+the reference's tests and networkx's results on the reference's catalog, the
+messy export case and the property-test graphs (tests/golden/).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+import graphs
+
+
+def csr(g):
+    return np.asarray(g["offsets"], dtype=np.uint32), np.asarray(g["targets"], dtype=np.uint32)
+
+
+def test_oracle_triangles_match_networkx(golden_graphs):
+    for g in golden_graphs:
+        o, t = csr(g)
+        assert O.triangle_count(o, t) == g["triangles"], g["name"]
+        # Same graph through the degree-oriented builder (correctness.rs:240-257).
+        pairs = [(u, v) for u in range(g["num_nodes"]) for v in t[o[u]:o[u + 1]] if v > u]
+        oo, ot = O.from_edge_pairs_oriented(pairs, g["num_nodes"])
+        assert O.triangle_count_oriented(oo, ot) == g["triangles"], g["name"]
+
+
+def test_oracle_bfs_matches_networkx_from_every_source(golden_graphs):
+    for g in golden_graphs:
+        o, t = csr(g)
+        for rec in g["bfs"]:
+            r = O.bfs(o, t, rec["source"])
+            assert r["distances"].tolist() == rec["distances"], (g["name"], rec["source"])
+            assert r["reachable"] == rec["reachable"]
+            assert r["max_depth"] == rec["max_depth"]
+
+
+def test_oracle_pagerank_matches_networkx_fixed_point(golden_graphs):
+    for g in golden_graphs:
+        if g["num_nodes"] == 0:
+            continue
+        o, t = csr(g)
+        r = O.pagerank(o, t, 0.85, 100000, 1e-15, rule="max")
+        assert r["converged"], g["name"]
+        np.testing.assert_allclose(r["ranks"], g["pagerank"], atol=1e-10, rtol=0, err_msg=g["name"])
+        assert abs(r["ranks"].sum() - 1.0) < 1e-12
+
+
+def test_oracle_k_truss_matches_networkx(golden_graphs):
+    for g in golden_graphs:
+        o, t = csr(g)
+        for k in range(3, 9):
+            r = O.k_truss(o, t, k)
+            got = sorted(map(tuple, r["edges"].tolist()))
+            assert len(set(got)) == len(got), (g["name"], k)
+            assert got == [tuple(e) for e in g["k_truss"][str(k)]], (g["name"], k)
+
+
+def test_oracle_reproduces_reference_literal_answers(pins):
+    k4o, k4t = graphs.K4_CSR
+    p5o, p5t = graphs.PATH5_CSR
+    lookup = {"K4": (k4o, k4t), "path5": (p5o, p5t)}
+    k5o, k5t = O.from_edge_pairs(graphs.complete_edges(5), 5, True)
+    lookup["K5"] = (k5o, k5t)
+    for pin in pins["triangles"]:
+        if pin["graph"] == "K5 oriented":
+            oo, ot = O.from_edge_pairs_oriented(graphs.complete_edges(5), 5)
+            assert O.triangle_count_oriented(oo, ot) == pin["value"]
+        else:
+            assert O.triangle_count(*lookup[pin["graph"]]) == pin["value"], pin
+    p6 = O.from_edge_pairs(graphs.path_edges(6), 6, True)
+    lookup["path6"] = p6
+    lookup["edgeless3"] = ([0, 0, 0, 0], [])
+    for pin in pins["bfs"]:
+        r = O.bfs(*lookup[pin["graph"]], pin["source"])
+        if "distances" in pin:
+            assert r["distances"].tolist() == pin["distances"]
+        assert r["reachable"] == pin["reachable"] and r["max_depth"] == pin["max_depth"], pin
+    lookup["empty"] = ([0], [])
+    for pin in pins["pagerank"]:
+        r = O.pagerank(*lookup[pin["graph"]], pin["damping"], pin["max_iterations"], pin["tolerance"])
+        if "value" in pin:
+            assert np.all(np.abs(r["ranks"] - pin["value"]) < pin["abs_tol"]), pin
+        if "ranks" in pin:
+            assert r["ranks"].tolist() == pin["ranks"]
+        if "converged" in pin:
+            assert r["converged"] == pin["converged"]
+    lookup["edgeless4"] = ([0, 0, 0, 0, 0], [])
+    for pin in pins["k_truss"]:
+        assert len(O.k_truss(*lookup[pin["graph"]], pin["k"])["edges"]) == pin["edges"], pin
+
+
+def test_oracle_builders_match_reference_examples(pins):
+    for b in pins["builders"]:
+        if b["call"] == "from_edge_pairs":
+            o, t = O.from_edge_pairs(b["edges"], b["num_nodes"], b["symmetric"])
+        else:
+            o, t = O.from_edge_pairs_oriented(b["edges"], b["num_nodes"])
+        assert o.tolist() == b["offsets"] and t.tolist() == b["targets"], b
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_oracle_oriented_builder_rules(seed):
+    """csr_export.rs(tests):402-458: each edge once, lower (degree, id) -> higher,
+    and the oriented count equals a brute-force triangle count."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(1, 14))
+    raw = rng.integers(0, n, size=(int(rng.integers(0, 60)), 2))
+    o, t = O.from_edge_pairs_oriented(raw, n)
+    und = {(min(a, b), max(a, b)) for a, b in raw.tolist() if a != b}
+    assert len(t) == len(und)
+    deg = np.zeros(n, dtype=int)
+    for a, b in und:
+        deg[a] += 1
+        deg[b] += 1
+    seen = set()
+    for u in range(n):
+        for v in t[o[u]:o[u + 1]].tolist():
+            assert deg[u] < deg[v] or (deg[u] == deg[v] and u < v)
+            assert (min(u, v), max(u, v)) not in seen
+            seen.add((min(u, v), max(u, v)))
+    assert seen == und
+    brute = sum(
+        1
+        for a in range(n)
+        for b in range(a + 1, n)
+        for c in range(b + 1, n)
+        if (a, b) in und and (b, c) in und and (a, c) in und
+    )
+    assert O.triangle_count_oriented(o, t) == brute
+
+
+def test_oracle_k_truss_round_semantics_on_self_loops():
+    """A self-loop inflates first-round support (the reference merges raw lists,
+    kernels/k_truss.cu:59-92); the fixpoint is still the maximal k-truss."""
+    # Triangle 0-1-2 plus a pendant edge 2-3 with a self-loop at 3 and at 2.
+    o, t = O.from_edge_pairs([(0, 1), (1, 2), (0, 2), (2, 3), (3, 3), (2, 2)], 4, True)
+    r = O.k_truss(o, t, 3)
+    assert sorted(map(tuple, r["edges"].tolist())) == [(0, 1), (0, 2), (1, 2)]
+    # Edge 2-3 is kept in round 1 (self-loops at 2 and 3 count as common
+    # neighbours), loses the self-loops in round 1, and goes in round 2.
+    assert r["iterations"] == 3
