@@ -206,38 +206,6 @@ __global__ void __launch_bounds__(kBuThreads) bfs_bottomup_kernel(
     }
 }
 
-// Symmetry test: every entry u -> v needs v -> u. A warp walks 32 rows; the
-// lanes stride over each row and binary-search u in the neighbour's list.
-__global__ void csr_symmetry_kernel(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
-                                    uint32_t V, uint32_t* __restrict__ asymmetric) {
-    const unsigned lane = lane_id();
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
-        const uint32_t count = static_cast<uint32_t>(min_u64(32, V - base));
-        uint32_t s = 0, e = 0;
-        if (lane < count) {
-            s = offsets[base + lane];
-            e = offsets[base + lane + 1];
-        }
-        bool bad = false;
-        for (uint32_t i = 0; i < count; ++i) {
-            const uint32_t u = static_cast<uint32_t>(base + i);
-            const uint32_t start = __shfl_sync(kFullMask, s, i), end = __shfl_sync(kFullMask, e, i);
-            for (uint32_t j = start + lane; j < end; j += 32) {
-                const uint32_t v = targets[j];
-                const uint32_t vs = offsets[v], ve = offsets[v + 1];
-                const uint32_t p = lower_bound_u32(targets, vs, ve, u);
-                if (p == ve || targets[p] != u) bad = true;
-            }
-        }
-        if (__any_sync(kFullMask, bad)) {
-            if (lane == 0) atomicOr(asymmetric, 1u);
-            return;
-        }
-    }
-}
-
 // ---------------------------------------------------------------- host
 
 static Error ensure_work(GraphImpl& g) {
@@ -255,21 +223,10 @@ static Error ensure_work(GraphImpl& g) {
     GCU_TRY(w->counters.allocate(dev, 1));
     GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&w->host_counters), sizeof(BfsCounters)), "cudaMallocHost");
     // Bottom-up steps read in-neighbours; they equal the CSR lists only when
-    // the CSR is symmetric, so check once per graph.
-    if (g.num_edges == 0) {
-        w->symmetric = 1;
-    } else {
-        GCU_CUDA(cudaMemsetAsync(w->counters.ptr, 0, sizeof(BfsCounters), dev.stream), "memset");
-        unsigned blocks = static_cast<unsigned>(
-            std::min<uint64_t>(ceil_div_u64(g.num_nodes, 256), static_cast<uint64_t>(dev.sm_count) * 16));
-        GCU_LAUNCH(dev, "csr_symmetry", csr_symmetry_kernel, blocks, 256, 0, g.offsets.ptr, g.targets.ptr,
-                   g.num_nodes, reinterpret_cast<uint32_t*>(w->counters.ptr));
-        GCU_CUDA(cudaMemcpyAsync(w->host_counters, w->counters.ptr, sizeof(BfsCounters), cudaMemcpyDeviceToHost,
-                                 dev.stream),
-                 "copy");
-        GCU_TRY(dev.sync());
-        w->symmetric = w->host_counters->discovered == 0 ? 1 : 0;
-    }
+    // the CSR is symmetric (checked once per graph).
+    bool sym = false;
+    GCU_TRY(graph_symmetry(g, &sym));
+    w->symmetric = sym ? 1 : 0;
     g.bfs_work = w.release();
     return ok();
 }

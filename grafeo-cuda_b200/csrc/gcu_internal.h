@@ -163,6 +163,7 @@ struct GraphImpl {
     DeviceBuffer<uint32_t> offsets;
     DeviceBuffer<uint32_t> targets;
     std::mutex mu;  // guards the lazily built caches below
+    int symmetric = -1;  // every entry u -> v has v -> u: -1 unknown, 0 no, 1 yes
     PageRankPlan* pr_plan = nullptr;  // owned; freed by destroy_pagerank_plan
     BfsWork* bfs_work = nullptr;      // owned; freed by destroy_bfs_work
     ~GraphImpl();
@@ -189,6 +190,9 @@ std::string describe_node_violation(uint32_t node, uint32_t start, uint32_t end,
 // Finds the first node that breaks a CSR rule on the device; UINT32_MAX if none.
 Error validate_csr_device(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets,
                           uint32_t num_nodes, uint32_t num_edges, uint32_t* first_bad_node);
+
+// Whether every entry u -> v has its reverse v -> u (cached on the graph).
+Error graph_symmetry(GraphImpl& g, bool* symmetric);
 
 Error triangle_count(GraphImpl& g, bool oriented, uint64_t* total);
 Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reachable,

@@ -170,9 +170,20 @@ __global__ void __launch_bounds__(kPrThreads) pr_tile_kernel(
         uint64_t r = static_cast<uint64_t>(r0) + k;
         s_off[k] = r <= V ? ld_stream(offsets + r) : 0xFFFFFFFFu;
     }
-    for (uint32_t k = threadIdx.x; k < nnz; k += kPrThreads) {
-        uint32_t u = ld_stream(targets + z0 + k);
-        s_val[k] = __ldg(contrib_in + u);
+    {
+        // All of this thread's target loads first, then all gathers, so every
+        // thread keeps kPrItems independent requests in flight.
+        uint32_t u[kPrItems];
+#pragma unroll
+        for (int q = 0; q < kPrItems; ++q) {
+            const uint32_t k = threadIdx.x + q * kPrThreads;
+            u[q] = k < nnz ? ld_stream(targets + z0 + k) : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < kPrItems; ++q) {
+            const uint32_t k = threadIdx.x + q * kPrThreads;
+            if (k < nnz) s_val[k] = __ldg(contrib_in + u[q]);
+        }
     }
     if (threadIdx.x == 0) s_defer_row = kNoRow;
     __syncthreads();

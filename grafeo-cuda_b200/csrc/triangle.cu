@@ -6,11 +6,15 @@
 // over hubs), runs a single-thread prefix sum, and refuses graphs with more
 // than 134,217,727 forward edges (launch.rs:27-35). Here:
 //
-//  1. Orientation (symmetric input): each undirected edge is kept once, from
-//     the endpoint of lower (degree, id) to the higher one, the same rule as
+//  1. Orientation: each undirected edge is kept once, from the endpoint of
+//     lower (degree, id) to the higher one, the same rule as
 //     from_edge_pairs_oriented (csr_export.rs:319-329). A count pass, a device
 //     scan and an order-preserving fill pass build the DAG CSR; self-loops
 //     drop out because the order is strict. Max out-degree becomes O(sqrt m).
+//     A CSR that is not symmetric is oriented by id alone (keep v > u): the
+//     count below is then exactly the reference's formula, the sum over
+//     entries u -> v, v > u, of |{w in N(u) ∩ N(v) : w > v}|
+//     (triangle_counting.cu:246-315), whatever the input.
 //  2. Counting: sum over DAG edges u -> v of |N+(u) ∩ N+(v)|, which counts
 //     every triangle exactly once. Vertex-centric: a warp stages N+(u) in
 //     shared memory, then walks the wedges (v, w), v in N+(u), w in N+(v), 32 at
@@ -33,14 +37,14 @@ constexpr uint32_t kTcWarpCap = 256;     // list entries staged per warp
 constexpr uint32_t kTcBatch = 8;         // vertices fetched per warp at a time
 constexpr uint32_t kTcBlockCapMax = 48 * 1024;  // entries staged per CTA for hubs (192 KB)
 
-__device__ __forceinline__ bool dag_keep(uint32_t u, uint32_t du, uint32_t v, uint32_t dv) {
-    return du < dv || (du == dv && u < v);
+__device__ __forceinline__ bool dag_keep(uint32_t u, uint32_t du, uint32_t v, uint32_t dv, bool by_degree) {
+    return by_degree ? (du < dv || (du == dv && u < v)) : u < v;
 }
 
 // Pass 1: out-degree of every vertex in the degree-oriented DAG.
 __global__ void __launch_bounds__(256) tc_orient_count_kernel(const uint32_t* __restrict__ offsets,
                                                               const uint32_t* __restrict__ targets, uint32_t V,
-                                                              uint32_t* __restrict__ out_deg) {
+                                                              bool by_degree, uint32_t* __restrict__ out_deg) {
     const unsigned lane = lane_id();
     const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
@@ -60,7 +64,7 @@ __global__ void __launch_bounds__(256) tc_orient_count_kernel(const uint32_t* __
             for (uint32_t j = start + lane; j < end; j += 32) {
                 const uint32_t v = ld_stream(targets + j);
                 const uint32_t dv = __ldg(offsets + v + 1) - __ldg(offsets + v);
-                kept += dag_keep(u, du, v, dv) ? 1u : 0u;
+                kept += dag_keep(u, du, v, dv, by_degree) ? 1u : 0u;
             }
             kept = warp_sum(kept);
             if (lane == i) mine = kept;
@@ -72,7 +76,7 @@ __global__ void __launch_bounds__(256) tc_orient_count_kernel(const uint32_t* __
 // Pass 2: write the kept neighbours in list order (still sorted by id).
 __global__ void __launch_bounds__(256) tc_orient_fill_kernel(const uint32_t* __restrict__ offsets,
                                                              const uint32_t* __restrict__ targets, uint32_t V,
-                                                             const uint32_t* __restrict__ dag_offsets,
+                                                             bool by_degree, const uint32_t* __restrict__ dag_offsets,
                                                              uint32_t* __restrict__ dag_targets) {
     const unsigned lane = lane_id();
     const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
@@ -97,7 +101,7 @@ __global__ void __launch_bounds__(256) tc_orient_fill_kernel(const uint32_t* __r
                 if (j < end) {
                     v = ld_stream(targets + j);
                     const uint32_t dv = __ldg(offsets + v + 1) - __ldg(offsets + v);
-                    keep = dag_keep(u, du, v, dv);
+                    keep = dag_keep(u, du, v, dv, by_degree);
                 }
                 const unsigned mask = __ballot_sync(kFullMask, keep);
                 if (keep) dag_targets[out + __popc(mask & ((1u << lane) - 1))] = v;
@@ -274,12 +278,14 @@ Error triangle_count(GraphImpl& g, bool oriented, uint64_t* total) {
         // self-loop entry u -> u contributes |N(u)| like in the reference.
         return count_dag(dev, g.offsets.ptr, g.targets.ptr, V, 1, total);
     }
+    bool symmetric = false;
+    GCU_TRY(graph_symmetry(g, &symmetric));
     DeviceBuffer<uint32_t> dag_offsets, dag_targets;
     GCU_TRY(dag_offsets.allocate(dev, static_cast<uint64_t>(V) + 1));
     const unsigned grid = static_cast<unsigned>(
         std::min<uint64_t>(ceil_div_u64(ceil_div_u64(V, 32) * 32, 256), static_cast<uint64_t>(dev.sm_count) * 16));
     GCU_LAUNCH(dev, "tc_orient_count", tc_orient_count_kernel, grid, 256, 0, g.offsets.ptr, g.targets.ptr, V,
-               dag_offsets.ptr);
+               symmetric, dag_offsets.ptr);
     GCU_TRY(exclusive_scan_u32(dev, dag_offsets.ptr, dag_offsets.ptr, V));
     uint32_t m = 0;
     GCU_CUDA(cudaMemcpyAsync(&m, dag_offsets.ptr + V, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
@@ -287,7 +293,7 @@ Error triangle_count(GraphImpl& g, bool oriented, uint64_t* total) {
     if (m == 0) return ok();
     GCU_TRY(dag_targets.allocate(dev, m));
     GCU_LAUNCH(dev, "tc_orient_fill", tc_orient_fill_kernel, grid, 256, 0, g.offsets.ptr, g.targets.ptr, V,
-               dag_offsets.ptr, dag_targets.ptr);
+               symmetric, dag_offsets.ptr, dag_targets.ptr);
     // A DAG vertex needs two out-neighbours to close a triangle.
     return count_dag(dev, dag_offsets.ptr, dag_targets.ptr, V, 2, total);
 }

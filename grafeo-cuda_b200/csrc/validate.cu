@@ -9,6 +9,8 @@
 //   offsets[node + 1] >= offsets[node]                 ("offsets decrease ...")
 //   every target < num_nodes                           ("... has neighbor ...")
 //   every list strictly increasing                     ("... not strictly increasing ...")
+#include <algorithm>
+
 #include "device_common.cuh"
 #include "gcu_internal.h"
 
@@ -70,6 +72,62 @@ Error validate_csr_device(DeviceImpl& dev, const uint32_t* d_offsets, const uint
     GCU_CUDA(cudaMemcpyAsync(&host, flag.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy flag");
     GCU_TRY(dev.sync());
     *first_bad_node = host;
+    return ok();
+}
+
+// Symmetry test: every entry u -> v needs v -> u. A warp walks 32 rows; the
+// lanes stride over each row and binary-search u in the neighbour's list.
+__global__ void csr_symmetry_kernel(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
+                                    uint32_t V, uint32_t* __restrict__ asymmetric) {
+    const unsigned lane = lane_id();
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
+        const uint32_t count = static_cast<uint32_t>(min_u64(32, V - base));
+        uint32_t s = 0, e = 0;
+        if (lane < count) {
+            s = offsets[base + lane];
+            e = offsets[base + lane + 1];
+        }
+        bool bad = false;
+        for (uint32_t i = 0; i < count; ++i) {
+            const uint32_t u = static_cast<uint32_t>(base + i);
+            const uint32_t start = __shfl_sync(kFullMask, s, i), end = __shfl_sync(kFullMask, e, i);
+            for (uint32_t j = start + lane; j < end; j += 32) {
+                const uint32_t v = targets[j];
+                const uint32_t vs = offsets[v], ve = offsets[v + 1];
+                const uint32_t p = lower_bound_u32(targets, vs, ve, u);
+                if (p == ve || targets[p] != u) bad = true;
+            }
+        }
+        if (__any_sync(kFullMask, bad)) {
+            if (lane == 0) atomicOr(asymmetric, 1u);
+            return;
+        }
+    }
+}
+
+
+Error graph_symmetry(GraphImpl& g, bool* symmetric) {
+    if (g.symmetric < 0) {
+        if (g.num_edges == 0) {
+            g.symmetric = 1;
+        } else {
+            DeviceImpl& dev = *g.dev;
+            DeviceBuffer<uint32_t> flag;
+            GCU_TRY(flag.allocate(dev, 1));
+            GCU_CUDA(cudaMemsetAsync(flag.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
+            unsigned blocks = static_cast<unsigned>(
+                std::min<uint64_t>(ceil_div_u64(g.num_nodes, 256), static_cast<uint64_t>(dev.sm_count) * 16));
+            GCU_LAUNCH(dev, "csr_symmetry", csr_symmetry_kernel, blocks, 256, 0, g.offsets.ptr, g.targets.ptr,
+                       g.num_nodes, flag.ptr);
+            uint32_t host = 0;
+            GCU_CUDA(cudaMemcpyAsync(&host, flag.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+            GCU_TRY(dev.sync());
+            g.symmetric = host == 0 ? 1 : 0;
+        }
+    }
+    *symmetric = g.symmetric == 1;
     return ok();
 }
 

@@ -180,6 +180,8 @@ void orc_pagerank(const uint32_t* offsets, const uint32_t* targets, uint32_t n, 
 size_t orc_k_truss(const uint32_t* offsets, const uint32_t* targets, uint32_t n, uint32_t k, uint32_t* out,
                    uint32_t* iterations) {
     const size_t E = offsets[n];
+    *iterations = 0;
+    if (E == 0) return 0; /* k_truss.rs:53-60: no edges, no rounds */
     uint8_t* removed = (uint8_t*)calloc(E ? E : 1, 1);
     uint32_t* support = (uint32_t*)malloc(sizeof(uint32_t) * (E ? E : 1));
     const uint32_t threshold = k - 2;
