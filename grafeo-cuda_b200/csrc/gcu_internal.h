@@ -194,6 +194,12 @@ Error validate_csr_device(DeviceImpl& dev, const uint32_t* d_offsets, const uint
 // Whether every entry u -> v has its reverse v -> u (cached on the graph).
 Error graph_symmetry(GraphImpl& g, bool* symmetric);
 
+// Degree-oriented (by_degree) or id-oriented DAG of the CSR: every undirected
+// edge once, lists still sorted. With `rev` (reverse-entry index) and dag_eid,
+// also the CSR index of each DAG edge's u < v entry. *m = DAG edges.
+Error build_dag(GraphImpl& g, bool by_degree, const uint32_t* rev, DeviceBuffer<uint32_t>* dag_offsets,
+                DeviceBuffer<uint32_t>* dag_targets, DeviceBuffer<uint32_t>* dag_eid, uint32_t* m);
+
 Error triangle_count(GraphImpl& g, bool oriented, uint64_t* total);
 Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reachable,
           int32_t* max_depth);

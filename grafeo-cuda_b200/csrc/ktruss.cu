@@ -1,28 +1,35 @@
 // k-truss by synchronous peeling.
 //
 // Reference: crates/grafeo-cuda-algos/src/k_truss.rs:42-161 and
-// kernels/k_truss.cu:46-124. Each round computes, for every live CSR entry
-// u -> v with v > u, support = |live N(u) ∩ live N(v)| (entry-level liveness, so
-// in the first round a live self-loop at u or v counts as a common neighbour
-// exactly as in the reference's merge), copies it to the live reverse entry
-// v -> u, and then removes every live entry whose support is below k - 2. The
-// rounds repeat until one removes nothing; the number of rounds is the
-// reference's `iterations`. Since every round sees the same live set as the
-// reference's round, removed sets and round counts are identical.
+// kernels/k_truss.cu:46-124. Each reference round computes, for every live CSR
+// entry u -> v with v > u, support = |live N(u) ∩ live N(v)| (entry-level
+// liveness, so in the first round a live self-loop at u or v counts as a
+// common neighbour, as the reference's merge of the raw lists does), copies it
+// to the live reverse entry v -> u, and then removes every live entry whose
+// support is below k - 2. Rounds repeat until one removes nothing; their count
+// is the reference's `iterations`. Two paths give exactly the same removed
+// sets round by round, hence the same edges and round count:
 //
-// Differences from the reference's kernels, same results:
-//  * a warp per entry intersects the two lists by walking the shorter one and
-//    binary-searching the longer (the reference merges both lists in one
-//    thread, per node);
-//  * the reverse entry comes from a precomputed index (the reference scans
-//    N(v) linearly for it every round);
-//  * the source vertex of every entry is materialised once (COO row array);
-//  * the result edge list is compacted on the device in CSR order (the
-//    reference copies removed/offsets/targets back and loops on the host).
+//  * Symmetric CSR (every graph exported from Grafeo): the support of every
+//    undirected edge is its triangle count, found once by enumerating the
+//    triangles of the degree-oriented DAG (wedge.cuh) with three atomic adds
+//    per triangle; round 1 adds one for a self-loop at either end. After a
+//    round removes a set R of edges, each triangle with an edge in R that was
+//    alive at the start of the round is destroyed once (credited to its
+//    removed edge with the smallest id) and its surviving edges lose one
+//    support, so the supports stay exact for the next round without
+//    recomputing them. Work per round is proportional to the edges removed.
+//  * Any other CSR: the reference's per-entry rules with all supports
+//    recomputed each round (a warp per entry, binary-search intersection).
+//
+// Both paths use a reverse-entry index instead of the reference's linear scan
+// of N(v), and compact the result edge list on the device in CSR order (the
+// reference copies removed/offsets/targets back and loops on the host).
 #include <algorithm>
 
 #include "device_common.cuh"
 #include "gcu_internal.h"
+#include "wedge.cuh"
 
 namespace gcu {
 
@@ -121,22 +128,260 @@ __global__ void kt_filter_kernel(const uint32_t* __restrict__ support, uint8_t* 
     if (lane_id() == 0 && mine) atomicAdd(removed, mine);
 }
 
-__global__ void kt_flag_kernel(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ src,
-                               const uint8_t* __restrict__ live, uint32_t E, uint32_t* __restrict__ flag) {
+struct LiveFlag {
+    const uint8_t* live;
+    __device__ __forceinline__ bool operator()(uint64_t j) const { return live[j] != 0; }
+};
+struct RoundState {
+    const uint32_t* state;  // 0 = alive, r = removed in round r
+    __device__ __forceinline__ bool operator()(uint64_t j) const { return state[j] == 0; }
+};
+
+template <class Alive>
+__global__ void kt_flag_kernel(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ src, Alive alive,
+                               uint32_t E, uint32_t* __restrict__ flag) {
     for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < E;
          j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        flag[j] = (live[j] && targets[j] > src[j]) ? 1u : 0u;
+        flag[j] = (targets[j] > src[j] && alive(j)) ? 1u : 0u;
     }
 }
 
-__global__ void kt_emit_kernel(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ src,
-                               const uint8_t* __restrict__ live, uint32_t E, const uint32_t* __restrict__ pos,
-                               uint2* __restrict__ out) {
+template <class Alive>
+__global__ void kt_emit_kernel(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ src, Alive alive,
+                               uint32_t E, const uint32_t* __restrict__ pos, uint2* __restrict__ out) {
     for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < E;
          j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint32_t u = src[j], v = targets[j];
-        if (live[j] && v > u) out[pos[j]] = make_uint2(u, v);
+        if (v > u && alive(j)) out[pos[j]] = make_uint2(u, v);
     }
+}
+
+// ---------------------------------------------------------------- symmetric CSR: incremental peeling
+
+namespace {
+
+// Adds each triangle found on the DAG to the support of its three edges.
+struct SupportSink {
+    static constexpr bool kNeedsPos = true;
+    const uint32_t* dag_eid;
+    uint32_t* support;
+    __device__ __forceinline__ void hit(uint32_t base, uint32_t pv, uint32_t pw, uint32_t evw) {
+        atomicAdd(support + dag_eid[base + pv], 1u);
+        atomicAdd(support + dag_eid[base + pw], 1u);
+        atomicAdd(support + dag_eid[evw], 1u);
+    }
+    __device__ __forceinline__ void finish() {}
+};
+
+}  // namespace
+
+// loop[u] = 1 for every vertex with a self-loop entry; counts them in *loops.
+__global__ void kt_loops_kernel(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ src, uint32_t E,
+                                uint8_t* __restrict__ loop, uint32_t* __restrict__ loops) {
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < E;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t u = src[j];
+        if (targets[j] == u) {
+            loop[u] = 1;
+            atomicAdd(loops, 1u);
+        }
+    }
+}
+
+// Round r: every alive u < v entry whose support is below the threshold is
+// removed (state = r) and listed. In round 1 a self-loop at either end adds
+// one to the support, as the reference's merge of the raw lists does.
+__global__ void kt_round_filter_kernel(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ src,
+                                       const uint8_t* __restrict__ loop, const uint32_t* __restrict__ support,
+                                       uint32_t* __restrict__ state, uint32_t E, uint32_t threshold, uint32_t round,
+                                       uint32_t* __restrict__ removed, uint32_t* __restrict__ removed_count) {
+    const unsigned lane = lane_id();
+    for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~31ull; base < E;
+         base += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t j = base + lane;
+        bool take = false;
+        if (j < E && state[j] == 0) {
+            const uint32_t u = src[j], v = targets[j];
+            if (v > u) {
+                uint32_t s = support[j];
+                if (round == 1) s += loop[u] + loop[v];
+                take = s < threshold;
+            }
+        }
+        const unsigned mask = __ballot_sync(kFullMask, take);
+        if (mask == 0) continue;
+        uint32_t at = 0;
+        const int leader = __ffs(mask) - 1;
+        if (lane == static_cast<unsigned>(leader)) at = atomicAdd(removed_count, static_cast<uint32_t>(__popc(mask)));
+        at = __shfl_sync(kFullMask, at, leader);
+        if (take) {
+            state[j] = round;
+            removed[at + __popc(mask & ((1u << lane) - 1))] = static_cast<uint32_t>(j);
+        }
+    }
+}
+
+// For every edge (a, b) removed in round r, every triangle {a, b, w} still
+// alive at the start of the round is destroyed: each of its edges that
+// survives the round loses one support. A triangle with several edges removed
+// in this round is handled once, by the removed edge with the smallest id.
+__global__ void __launch_bounds__(256) kt_peel_kernel(const uint32_t* __restrict__ offsets,
+                                                      const uint32_t* __restrict__ targets,
+                                                      const uint32_t* __restrict__ src,
+                                                      const uint32_t* __restrict__ rev,
+                                                      const uint32_t* __restrict__ state,
+                                                      uint32_t* __restrict__ support,
+                                                      const uint32_t* __restrict__ removed,
+                                                      const uint32_t* __restrict__ removed_count, uint32_t round) {
+    const unsigned lane = lane_id();
+    const uint32_t n = *removed_count;
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
+        const uint32_t e = removed[i];
+        const uint32_t a = src[e], b = targets[e];
+        uint32_t xs = offsets[a], xe = offsets[a + 1], ys = offsets[b], ye = offsets[b + 1];
+        uint32_t x = a, y = b;
+        if (xe - xs > ye - ys) {  // walk the shorter list, search the longer
+            uint32_t t = xs; xs = ys; ys = t;
+            t = xe; xe = ye; ye = t;
+            x = b;
+            y = a;
+        }
+        for (uint32_t p = xs + lane; p < xe; p += 32) {
+            const uint32_t w = targets[p];
+            if (w == a || w == b) continue;
+            const uint32_t e1 = x < w ? p : rev[p];
+            const uint32_t s1 = state[e1];
+            if (s1 != 0 && s1 != round) continue;
+            const uint32_t q = lower_bound_u32(targets, ys, ye, w);
+            if (q == ye || targets[q] != w) continue;
+            const uint32_t e2 = y < w ? q : rev[q];
+            const uint32_t s2 = state[e2];
+            if (s2 != 0 && s2 != round) continue;
+            if ((s1 == round && e1 < e) || (s2 == round && e2 < e)) continue;
+            if (s1 == 0) atomicSub(support + e1, 1u);
+            if (s2 == 0) atomicSub(support + e2, 1u);
+        }
+    }
+}
+
+// Compacts the alive u < v entries, in CSR order, into host pairs.
+template <class Alive>
+static Error emit_edges(DeviceImpl& dev, GraphImpl& g, const uint32_t* src, Alive alive, uint32_t* flag,
+                        uint32_t* pos, std::vector<uint32_t>* edges) {
+    const uint32_t E = g.num_edges;
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
+    GCU_LAUNCH(dev, "kt_flag", kt_flag_kernel<Alive>, edge_grid, 256, 0, g.targets.ptr, src, alive, E, flag);
+    GCU_TRY(exclusive_scan_u32(dev, flag, pos, E));
+    uint32_t count = 0;
+    GCU_CUDA(cudaMemcpyAsync(&count, pos + E, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+    GCU_TRY(dev.sync());
+    if (count > 0) {
+        DeviceBuffer<uint2> out;
+        GCU_TRY(out.allocate(dev, count));
+        GCU_LAUNCH(dev, "kt_emit", kt_emit_kernel<Alive>, edge_grid, 256, 0, g.targets.ptr, src, alive, E, pos,
+                   out.ptr);
+        edges->resize(2 * static_cast<size_t>(count));
+        GCU_CUDA(cudaMemcpyAsync(edges->data(), out.ptr, sizeof(uint2) * count, cudaMemcpyDeviceToHost, dev.stream),
+                 "copy edges to host");
+        GCU_TRY(dev.sync());
+    }
+    return ok();
+}
+
+// Any CSR: the reference's rounds, recomputing every support each round.
+static Error k_truss_general(GraphImpl& g, uint32_t k, const uint32_t* src, const uint32_t* rev,
+                             std::vector<uint32_t>* edges, uint32_t* iterations) {
+    DeviceImpl& dev = *g.dev;
+    const uint32_t E = g.num_edges;
+    const uint32_t threshold = k - 2;
+    DeviceBuffer<uint32_t> support, pos, scratch;
+    DeviceBuffer<uint8_t> live;
+    GCU_TRY(support.allocate(dev, E));
+    GCU_TRY(pos.allocate(dev, static_cast<uint64_t>(E) + 1));
+    GCU_TRY(live.allocate(dev, E));
+    GCU_TRY(scratch.allocate(dev, 1));
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
+    GCU_CUDA(cudaMemsetAsync(live.ptr, 1, E, dev.stream), "memset");
+    uint32_t rounds = 0;
+    while (true) {
+        GCU_CUDA(cudaMemsetAsync(support.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
+        GCU_LAUNCH(dev, "kt_support", kt_support_kernel, edge_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src, rev,
+                   live.ptr, E, support.ptr);
+        GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
+        GCU_LAUNCH(dev, "kt_filter", kt_filter_kernel, edge_grid, 256, 0, support.ptr, live.ptr, E, threshold,
+                   scratch.ptr);
+        uint32_t removed = 0;
+        GCU_CUDA(cudaMemcpyAsync(&removed, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+        GCU_TRY(dev.sync());
+        rounds += 1;
+        if (removed == 0) break;
+    }
+    *iterations = rounds;
+    return emit_edges(dev, g, src, LiveFlag{live.ptr}, support.ptr, pos.ptr, edges);
+}
+
+// Symmetric CSR: per-edge triangle counts from the DAG, then incremental
+// peeling. Every round removes exactly the entries the reference's round
+// removes, so the edge list and the round count are the same.
+static Error k_truss_symmetric(GraphImpl& g, uint32_t k, const uint32_t* src, const uint32_t* rev,
+                               std::vector<uint32_t>* edges, uint32_t* iterations) {
+    DeviceImpl& dev = *g.dev;
+    const uint32_t E = g.num_edges, V = g.num_nodes;
+    const uint32_t threshold = k - 2;
+    DeviceBuffer<uint32_t> support, state, removed, scratch;
+    DeviceBuffer<uint8_t> loop;
+    GCU_TRY(support.allocate(dev, static_cast<uint64_t>(E) + 1));
+    GCU_TRY(state.allocate(dev, static_cast<uint64_t>(E) + 1));
+    GCU_TRY(removed.allocate(dev, E));
+    GCU_TRY(loop.allocate(dev, V));
+    GCU_TRY(scratch.allocate(dev, 2));  // [0] removed this round, [1] self-loops
+    GCU_CUDA(cudaMemsetAsync(support.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(state.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(loop.ptr, 0, V, dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, 2 * sizeof(uint32_t), dev.stream), "memset");
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
+    GCU_LAUNCH(dev, "kt_loops", kt_loops_kernel, edge_grid, 256, 0, g.targets.ptr, src, E, loop.ptr, scratch.ptr + 1);
+
+    // Support = triangles per undirected edge, counted on the degree DAG.
+    {
+        DeviceBuffer<uint32_t> dag_offsets, dag_targets, dag_eid;
+        uint32_t m = 0;
+        GCU_TRY(build_dag(g, true, rev, &dag_offsets, &dag_targets, &dag_eid, &m));
+        if (m > 0) {
+            GCU_TRY(run_wedges(dev, dag_offsets.ptr, dag_targets.ptr, V, 2, SupportSink{dag_eid.ptr, support.ptr},
+                               "kt"));
+        }
+    }
+    uint32_t loops = 0;
+    GCU_CUDA(cudaMemcpyAsync(&loops, scratch.ptr + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+    GCU_TRY(dev.sync());
+
+    uint32_t round = 1;
+    while (true) {
+        GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
+        GCU_LAUNCH(dev, "kt_round_filter", kt_round_filter_kernel, edge_grid, 256, 0, g.targets.ptr, src, loop.ptr,
+                   support.ptr, state.ptr, E, threshold, round, removed.ptr, scratch.ptr);
+        uint32_t n = 0;
+        GCU_CUDA(cudaMemcpyAsync(&n, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+        GCU_TRY(dev.sync());
+        // Round 1 also removes the self-loop entries (their support is 0).
+        const bool removed_any = n > 0 || (round == 1 && loops > 0);
+        if (!removed_any) break;
+        if (n > 0) {
+            const unsigned peel_grid =
+                static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(static_cast<uint64_t>(n) * 32, 256), cap));
+            GCU_LAUNCH(dev, "kt_peel", kt_peel_kernel, peel_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src, rev,
+                       state.ptr, support.ptr, removed.ptr, scratch.ptr, round);
+        }
+        round += 1;
+    }
+    *iterations = round;
+    // `removed` (E entries) and `support` (E + 1) are reused as the compaction's flag and scan buffers.
+    return emit_edges(dev, g, src, RoundState{state.ptr}, removed.ptr, support.ptr, edges);
 }
 
 Error k_truss(GraphImpl& g, uint32_t k, std::vector<uint32_t>* edges, uint32_t* iterations) {
@@ -146,61 +391,19 @@ Error k_truss(GraphImpl& g, uint32_t k, std::vector<uint32_t>* edges, uint32_t* 
     // k_truss.rs:53-60: no edges, no truss.
     if (E == 0) return ok();
     DeviceImpl& dev = *g.dev;
-    const uint32_t threshold = k - 2;
-    DeviceBuffer<uint32_t> src, rev, support, scratch;
-    DeviceBuffer<uint8_t> live;
+    bool symmetric = false;
+    GCU_TRY(graph_symmetry(g, &symmetric));
+    DeviceBuffer<uint32_t> src, rev;
     GCU_TRY(src.allocate(dev, E));
-    GCU_TRY(rev.allocate(dev, static_cast<uint64_t>(E) + 1));  // + 1: reused as scan output
-    GCU_TRY(support.allocate(dev, E));
-    GCU_TRY(live.allocate(dev, E));
-    GCU_TRY(scratch.allocate(dev, 2));
-    uint32_t* host = nullptr;
-    GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host), sizeof(uint32_t)), "cudaMallocHost");
-    struct HostFree {
-        uint32_t* p;
-        ~HostFree() { cudaFreeHost(p); }
-    } host_guard{host};
-
+    GCU_TRY(rev.allocate(dev, E));
     const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
     const unsigned row_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
     const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
     GCU_LAUNCH(dev, "kt_rows", kt_rows_kernel, row_grid, 256, 0, g.offsets.ptr, V, src.ptr);
     GCU_LAUNCH(dev, "kt_reverse", kt_reverse_kernel, edge_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src.ptr, E,
                rev.ptr);
-    GCU_CUDA(cudaMemsetAsync(live.ptr, 1, E, dev.stream), "memset");
-
-    uint32_t rounds = 0;
-    while (true) {
-        GCU_CUDA(cudaMemsetAsync(support.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
-        GCU_LAUNCH(dev, "kt_support", kt_support_kernel, edge_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src.ptr,
-                   rev.ptr, live.ptr, E, support.ptr);
-        GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
-        GCU_LAUNCH(dev, "kt_filter", kt_filter_kernel, edge_grid, 256, 0, support.ptr, live.ptr, E, threshold,
-                   scratch.ptr);
-        GCU_CUDA(cudaMemcpyAsync(host, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
-        GCU_TRY(dev.sync());
-        rounds += 1;
-        if (*host == 0) break;
-    }
-
-    // Compact the surviving u < v entries in CSR order.
-    GCU_LAUNCH(dev, "kt_flag", kt_flag_kernel, edge_grid, 256, 0, g.targets.ptr, src.ptr, live.ptr, E, support.ptr);
-    GCU_TRY(exclusive_scan_u32(dev, support.ptr, rev.ptr, E));  // rev is free now
-    uint32_t count = 0;
-    GCU_CUDA(cudaMemcpyAsync(&count, rev.ptr + E, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
-    GCU_TRY(dev.sync());
-    if (count > 0) {
-        DeviceBuffer<uint2> out;
-        GCU_TRY(out.allocate(dev, count));
-        GCU_LAUNCH(dev, "kt_emit", kt_emit_kernel, edge_grid, 256, 0, g.targets.ptr, src.ptr, live.ptr, E, rev.ptr,
-                   out.ptr);
-        edges->resize(2 * static_cast<size_t>(count));
-        GCU_CUDA(cudaMemcpyAsync(edges->data(), out.ptr, sizeof(uint2) * count, cudaMemcpyDeviceToHost, dev.stream),
-                 "copy edges to host");
-        GCU_TRY(dev.sync());
-    }
-    *iterations = rounds;
-    return ok();
+    if (symmetric) return k_truss_symmetric(g, k, src.ptr, rev.ptr, edges, iterations);
+    return k_truss_general(g, k, src.ptr, rev.ptr, edges, iterations);
 }
 
 }  // namespace gcu

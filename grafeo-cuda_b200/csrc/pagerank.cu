@@ -38,6 +38,11 @@ constexpr int kPrItems = 8;                       // merge items per thread
 constexpr int kPrTile = kPrThreads * kPrItems;    // merge items per tile
 constexpr uint32_t kNoRow = 0xFFFFFFFFu;
 
+// Shared-memory index with one padding word per 32: each thread walks
+// kPrItems consecutive staged items, so without padding the lanes of a warp
+// would hit every 8th bank (an 8-way conflict on every merge step).
+__device__ __forceinline__ uint32_t pad(uint32_t k) { return k + (k >> 5); }
+
 struct PrState {
     double dangling;   // sum of ranks of dangling vertices in the current input ranks
     double last_diff;  // L1 change of the last iteration
@@ -150,8 +155,8 @@ __global__ void __launch_bounds__(kPrThreads) pr_tile_kernel(
     uint32_t* __restrict__ head_row, double* __restrict__ head_val, uint32_t* __restrict__ carry_row,
     double* __restrict__ carry_val, double* __restrict__ tile_diff, double* __restrict__ tile_dangle) {
     if (state->done) return;
-    __shared__ uint32_t s_off[kPrTile + 2];
-    __shared__ float s_val[kPrTile];
+    __shared__ uint32_t s_off[kPrTile + 2 + (kPrTile + 2) / 32 + 1];
+    __shared__ float s_val[kPrTile + kPrTile / 32];
     __shared__ double s_warp_v[kPrThreads / 32];
     __shared__ int s_warp_f[kPrThreads / 32];
     __shared__ uint32_t s_defer_row;
@@ -168,7 +173,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_tile_kernel(
     // Stage offsets[r0 .. r0 + nrows + 1] and the gathered contributions.
     for (uint32_t k = threadIdx.x; k < nrows + 2; k += kPrThreads) {
         uint64_t r = static_cast<uint64_t>(r0) + k;
-        s_off[k] = r <= V ? ld_stream(offsets + r) : 0xFFFFFFFFu;
+        s_off[pad(k)] = r <= V ? ld_stream(offsets + r) : 0xFFFFFFFFu;
     }
     {
         // All of this thread's target loads first, then all gathers, so every
@@ -182,7 +187,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_tile_kernel(
 #pragma unroll
         for (int q = 0; q < kPrItems; ++q) {
             const uint32_t k = threadIdx.x + q * kPrThreads;
-            if (k < nnz) s_val[k] = __ldg(contrib_in + u[q]);
+            if (k < nnz) s_val[pad(k)] = __ldg(contrib_in + u[q]);
         }
     }
     if (threadIdx.x == 0) s_defer_row = kNoRow;
@@ -193,7 +198,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_tile_kernel(
     uint32_t lo = dk > nnz ? dk - nnz : 0, hi = min(dk, nrows);
     while (lo < hi) {
         uint32_t p = (lo + hi) >> 1;
-        if (s_off[p + 1] <= z0 + dk - p - 1)
+        if (s_off[pad(p + 1)] <= z0 + dk - p - 1)
             lo = p + 1;
         else
             hi = p;
@@ -209,8 +214,8 @@ __global__ void __launch_bounds__(kPrThreads) pr_tile_kernel(
 #pragma unroll
     for (int q = 0; q < kPrItems; ++q) {
         if (dk + q >= stop) break;
-        if (jj < nnz && z0 + jj < s_off[rr + 1]) {
-            float y = s_val[jj] - comp;
+        if (jj < nnz && z0 + jj < s_off[pad(rr + 1)]) {
+            float y = s_val[pad(jj)] - comp;
             float s = acc + y;
             comp = (s - acc) - y;
             acc = s;
@@ -222,7 +227,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_tile_kernel(
                 head_partial = sum;
                 head_local = rr;
             } else {
-                pr_finish_row(r0 + rr, sum, s_off[rr + 1] - s_off[rr], rank_in, rank_out, contrib_out, base, damp,
+                pr_finish_row(r0 + rr, sum, s_off[pad(rr + 1)] - s_off[pad(rr)], rank_in, rank_out, contrib_out, base, damp,
                               spread, my_diff, my_dangle);
             }
             acc = 0.f;
@@ -274,11 +279,11 @@ __global__ void __launch_bounds__(kPrThreads) pr_tile_kernel(
         double total = head_partial + ex_v;
         uint32_t row = r0 + head_local;
         // The tile's first row began in an earlier tile: finish it in the fix-up.
-        if (!ex_f && s_off[0] < z0) {
+        if (!ex_f && s_off[pad(0)] < z0) {
             s_defer_row = row;
             s_defer_val = total;
         } else {
-            pr_finish_row(row, total, s_off[head_local + 1] - s_off[head_local], rank_in, rank_out, contrib_out,
+            pr_finish_row(row, total, s_off[pad(head_local + 1)] - s_off[pad(head_local)], rank_in, rank_out, contrib_out,
                           base, damp, spread, my_diff, my_dangle);
         }
     }

@@ -3,7 +3,7 @@
 // The reference checks every CSR on the host before the copy
 // (crates/grafeo-cuda-core/src/csr_export.rs:71-120): a serial O(V + E) scan
 // that takes longer than the algorithms themselves at scale. Here the arrays
-// are copied first and one coalesced pass on the device finds the first node
+// are copied first and coalesced passes on the device find the first node
 // that breaks a rule; the host then rebuilds the exact reference message for
 // that node alone (describe_node_violation). The rules, per node in order:
 //   offsets[node + 1] >= offsets[node]                 ("offsets decrease ...")
@@ -16,44 +16,51 @@
 
 namespace gcu {
 
-// One warp walks 32 consecutive nodes; for each node all lanes check its list
-// in coalesced 32-entry strides. The smallest offending node wins (atomicMin).
-__global__ void __launch_bounds__(256) csr_validate_kernel(const uint32_t* __restrict__ offsets,
-                                                           const uint32_t* __restrict__ targets,
-                                                           uint32_t num_nodes, uint32_t num_edges,
-                                                           uint32_t* __restrict__ first_bad) {
-    const unsigned lane = lane_id();
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t base = warp * 32; base < num_nodes; base += nwarps * 32) {
-        // Lane i loads the bounds of node base + i.
-        uint64_t my = base + lane;
-        uint32_t s = 0, e = 0;
-        if (my < num_nodes) {
-            s = offsets[my];
-            e = offsets[my + 1];
-        }
-        const uint32_t count = static_cast<uint32_t>(min_u64(32, num_nodes - base));
-        for (uint32_t i = 0; i < count; ++i) {
-            uint32_t start = __shfl_sync(kFullMask, s, i);
-            uint32_t end = __shfl_sync(kFullMask, e, i);
-            bool bad = end < start || end > num_edges;
-            if (!bad) {
-                for (uint32_t j = start + lane; j < end; j += 32) {
-                    uint32_t t = targets[j];
-                    bool wrong = t >= num_nodes || (j > start && targets[j - 1] >= t);
-                    if (__any_sync(__activemask(), wrong)) {
-                        bad = true;
-                        break;
-                    }
-                }
-                bad = __any_sync(kFullMask, bad);
-            }
-            if (bad) {
-                if (lane == 0) atomicMin(first_bad, static_cast<uint32_t>(base + i));
-                break;  // later nodes of this warp cannot be first
-            }
-        }
+// Three coalesced passes, each O(V) or O(E), with the smallest offending node
+// kept by atomicMin (flags[0..2] = decrease, past-the-end, list error):
+//  1. per node: offsets[u+1] < offsets[u] (decrease) or offsets[u+1] > E;
+//  2. per node below the first such node: mark the first entry of every
+//     non-empty list in a bitmap over the entries;
+//  3. per entry below that node's offset: target >= V, or not a list start
+//     and not above its predecessor; the offending entry's node is found by
+//     a binary search over the (monotone) offsets.
+// A node's own rules are checked before later nodes' ones, so the smallest
+// node reported is the first node the reference's serial scan would reject.
+__global__ void csr_check_offsets_kernel(const uint32_t* __restrict__ offsets, uint32_t V, uint32_t E,
+                                         uint32_t* __restrict__ flags) {
+    for (uint64_t u = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u < V;
+         u += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t s = offsets[u], e = offsets[u + 1];
+        if (e < s) atomicMin(flags + 0, static_cast<uint32_t>(u));
+        if (e > E) atomicMin(flags + 1, static_cast<uint32_t>(u));
+    }
+}
+
+__device__ __forceinline__ uint32_t checked_limit(const uint32_t* flags, uint32_t V) {
+    return min(min(flags[0], flags[1]), V);
+}
+
+__global__ void csr_mark_starts_kernel(const uint32_t* __restrict__ offsets, uint32_t V,
+                                       const uint32_t* __restrict__ flags, uint32_t* __restrict__ starts) {
+    const uint32_t limit = checked_limit(flags, V);
+    for (uint64_t u = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u < limit;
+         u += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t s = offsets[u];
+        if (offsets[u + 1] > s) atomicOr(starts + (s >> 5), 1u << (s & 31));
+    }
+}
+
+__global__ void csr_check_entries_kernel(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
+                                         uint32_t V, const uint32_t* __restrict__ starts,
+                                         uint32_t* __restrict__ flags) {
+    const uint32_t limit = checked_limit(flags, V);
+    const uint32_t end = offsets[limit];
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < end;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t t = ld_stream(targets + j);
+        const bool first = (starts[j >> 5] >> (j & 31)) & 1u;
+        const bool bad = t >= V || (!first && targets[j - 1] >= t);
+        if (bad) atomicMin(flags + 2, row_of_entry(offsets, limit, static_cast<uint32_t>(j)));
     }
 }
 
@@ -61,17 +68,26 @@ Error validate_csr_device(DeviceImpl& dev, const uint32_t* d_offsets, const uint
                           uint32_t num_nodes, uint32_t num_edges, uint32_t* first_bad_node) {
     *first_bad_node = UINT32_MAX;
     if (num_nodes == 0) return ok();
-    DeviceBuffer<uint32_t> flag;
-    GCU_TRY(flag.allocate(dev, 1));
-    GCU_CUDA(cudaMemsetAsync(flag.ptr, 0xFF, sizeof(uint32_t), dev.stream), "memset");
-    uint64_t warps = ceil_div_u64(num_nodes, 32);
-    uint64_t blocks = std::min<uint64_t>(ceil_div_u64(warps * 32, 256), static_cast<uint64_t>(dev.sm_count) * 16);
-    GCU_LAUNCH(dev, "csr_validate", csr_validate_kernel, static_cast<unsigned>(blocks), 256, 0, d_offsets,
-               d_targets, num_nodes, num_edges, flag.ptr);
-    uint32_t host = UINT32_MAX;
-    GCU_CUDA(cudaMemcpyAsync(&host, flag.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy flag");
+    const uint64_t words = ceil_div_u64(num_edges, 32);
+    DeviceBuffer<uint32_t> scratch;  // 4 flags, then the list-start bitmap
+    GCU_TRY(scratch.allocate(dev, 4 + words));
+    uint32_t* flags = scratch.ptr;
+    uint32_t* starts = scratch.ptr + 4;
+    GCU_CUDA(cudaMemsetAsync(flags, 0xFF, 4 * sizeof(uint32_t), dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(starts, 0, words * sizeof(uint32_t), dev.stream), "memset");
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned node_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(num_nodes, 256), cap));
+    const unsigned entry_grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(num_edges, 256), cap)));
+    GCU_LAUNCH(dev, "csr_check_offsets", csr_check_offsets_kernel, node_grid, 256, 0, d_offsets, num_nodes, num_edges,
+               flags);
+    GCU_LAUNCH(dev, "csr_mark_starts", csr_mark_starts_kernel, node_grid, 256, 0, d_offsets, num_nodes, flags,
+               starts);
+    GCU_LAUNCH(dev, "csr_check_entries", csr_check_entries_kernel, entry_grid, 256, 0, d_offsets, d_targets,
+               num_nodes, starts, flags);
+    uint32_t host[4];
+    GCU_CUDA(cudaMemcpyAsync(host, flags, sizeof(host), cudaMemcpyDeviceToHost, dev.stream), "copy flags");
     GCU_TRY(dev.sync());
-    *first_bad_node = host;
+    *first_bad_node = std::min(std::min(host[0], host[1]), host[2]);
     return ok();
 }
 

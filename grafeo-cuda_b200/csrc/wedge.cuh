@@ -1,0 +1,251 @@
+// Wedge enumeration over a DAG CSR with shared-memory hash tables.
+//
+// Shared by triangle counting and k-truss support counting. For a vertex u
+// with out-list N+(u), the keys of N+(u) go into an open-addressing hash table
+// in shared memory (multiplicative hashing, linear probing, load <= 1/2), then
+// every wedge (v, w), v in N+(u), w in N+(v), is probed: a hit is a triangle
+// {u, v, w}. The wedges of up to 32 v's at a time are spread evenly over the
+// lanes of a warp by a warp scan of the d+(v) (a load-balanced search), so the
+// reads of the N+(v) lists are coalesced and no lane idles on short lists.
+#pragma once
+
+#include <algorithm>
+
+#include "device_common.cuh"
+#include "gcu_internal.h"
+
+namespace gcu {
+
+constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
+constexpr uint32_t kNotFound = 0xFFFFFFFFu;
+
+// Smallest b >= 6 with 2^b >= 2n: a table of 2^b slots at load <= 1/2.
+__host__ __device__ __forceinline__ uint32_t table_bits(uint32_t n) {
+    uint32_t b = 6;
+    while ((1u << b) < 2 * n) ++b;
+    return b;
+}
+
+__device__ __forceinline__ uint32_t hash_home(uint32_t key, uint32_t bits) {
+    return (key * 2654435761u) >> (32 - bits);
+}
+
+// Inserts a key that is not yet present. Keys are distinct (sorted lists), so
+// only the slot claim needs an atomic. Gives up after one sweep of the table,
+// which cannot happen below load 1.
+template <bool kWithPos>
+__device__ __forceinline__ void hash_insert(uint32_t* keys, uint32_t* pos, uint32_t bits, uint32_t key,
+                                            uint32_t value) {
+    const uint32_t mask = (1u << bits) - 1;
+    uint32_t s = hash_home(key, bits);
+    for (uint32_t i = 0; i <= mask; ++i) {
+        if (atomicCAS(keys + s, kEmptyKey, key) == kEmptyKey) {
+            if (kWithPos) pos[s] = value;
+            return;
+        }
+        s = (s + 1) & mask;
+    }
+}
+
+// Position stored with `key`, kNotFound if absent (1 when kWithPos is false
+// and the key is present).
+template <bool kWithPos>
+__device__ __forceinline__ uint32_t hash_find(const uint32_t* keys, const uint32_t* pos, uint32_t bits,
+                                              uint32_t key) {
+    const uint32_t mask = (1u << bits) - 1;
+    uint32_t s = hash_home(key, bits);
+    for (uint32_t i = 0; i <= mask; ++i) {
+        const uint32_t k = keys[s];
+        if (k == key) return kWithPos ? pos[s] : 1u;
+        if (k == kEmptyKey) return kNotFound;
+        s = (s + 1) & mask;
+    }
+    return kNotFound;
+}
+
+// Position of w in the sorted list a[0, n) or kNotFound (for lists too long
+// for a shared-memory table).
+__device__ __forceinline__ uint32_t sorted_find(const uint32_t* a, uint32_t n, uint32_t w) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t x = a[mid];
+        if (x < w)
+            lo = mid + 1;
+        else if (x > w)
+            hi = mid;
+        else
+            return mid;
+    }
+    return kNotFound;
+}
+
+// Walks the wedges of the out-neighbours v = list[c .. c + 31] of u (list =
+// N+(u), du entries); for every w in N+(v) that find(w) locates in N+(u) calls
+// hit(pos_v, pos_w, entry_vw): positions of v and w in N+(u) and the CSR entry
+// index of v -> w. s_excl / s_start are 32-word per-warp scratch.
+template <class Find, class Hit>
+__device__ __forceinline__ void wedge_chunk(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
+                                            const uint32_t* list, uint32_t du, uint32_t c, uint32_t* s_excl,
+                                            uint32_t* s_start, Find find, Hit hit) {
+    const unsigned lane = lane_id();
+    uint32_t vs = 0, dv = 0;
+    if (c + lane < du) {
+        const uint32_t v = list[c + lane];
+        vs = offsets[v];
+        dv = offsets[v + 1] - vs;
+    }
+    const uint32_t inc = warp_inclusive_scan(dv);
+    const uint32_t total = __shfl_sync(kFullMask, inc, 31);
+    __syncwarp();
+    s_excl[lane] = inc - dv;
+    s_start[lane] = vs;
+    __syncwarp();
+    for (uint32_t k = lane; k < total; k += 32) {
+        uint32_t lo = 0, hi = 32;  // largest j with s_excl[j] <= k (the v owning wedge k)
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (s_excl[mid] <= k)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const uint32_t entry = s_start[lo] + (k - s_excl[lo]);
+        const uint32_t p = find(targets[entry]);
+        if (p != kNotFound) hit(c + lo, p, entry);
+    }
+}
+
+// ---------------------------------------------------------------- kernels
+
+constexpr int kWedgeThreads = 256;
+constexpr int kWedgeWarps = kWedgeThreads / 32;
+constexpr uint32_t kWarpMaxDeg = 128;   // warp kernel: out-lists up to this length
+constexpr uint32_t kWarpSlots = 256;    // hash slots per warp (load <= 1/2)
+constexpr uint32_t kCtaMaxDeg = 2048;   // CTA kernel: hash table up to this length
+constexpr uint32_t kCtaSlots = 4096;
+constexpr uint32_t kVertexBatch = 8;    // vertices fetched per warp at a time
+
+// A Sink receives every triangle: hit(row_base, pos_v, pos_w, entry_vw) with
+// row_base = offsets[u] (so row_base + pos_v is the entry u -> v) and
+// finish() once per thread at the end. Sink::kNeedsPos says whether the hash
+// table has to keep the positions of the keys.
+
+// Warp per vertex for out-lists of [min_deg, kWarpMaxDeg] entries; vertices
+// are handed out dynamically kVertexBatch at a time.
+template <class Sink>
+__global__ void __launch_bounds__(kWedgeThreads) wedge_warp_kernel(const uint32_t* __restrict__ offsets,
+                                                                   const uint32_t* __restrict__ targets, uint32_t V,
+                                                                   uint32_t min_deg, uint32_t* __restrict__ next_vertex,
+                                                                   Sink sink) {
+    constexpr bool kPos = Sink::kNeedsPos;
+    __shared__ uint32_t s_keys[kWedgeWarps][kWarpSlots];
+    __shared__ uint32_t s_pos[kPos ? kWedgeWarps : 1][kPos ? kWarpSlots : 1];
+    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_start[kWedgeWarps][32];
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    uint32_t* keys = s_keys[warp];
+    uint32_t* pos = kPos ? s_pos[warp] : nullptr;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(next_vertex, kVertexBatch);
+        base = __shfl_sync(kFullMask, base, 0);
+        if (base >= V) break;
+        const uint32_t last = min(base + kVertexBatch, V);
+        for (uint32_t u = base; u < last; ++u) {
+            const uint32_t s = offsets[u], du = offsets[u + 1] - s;
+            if (du < min_deg || du > kWarpMaxDeg) continue;
+            const uint32_t bits = table_bits(du);
+            __syncwarp();
+            for (uint32_t k = lane; k < (1u << bits); k += 32) keys[k] = kEmptyKey;
+            __syncwarp();
+            for (uint32_t k = lane; k < du; k += 32) hash_insert<kPos>(keys, pos, bits, targets[s + k], k);
+            __syncwarp();
+            for (uint32_t c = 0; c < du; c += 32)
+                wedge_chunk(
+                    offsets, targets, targets + s, du, c, s_excl[warp], s_start[warp],
+                    [&](uint32_t w) { return hash_find<kPos>(keys, pos, bits, w); },
+                    [&](uint32_t pv, uint32_t pw, uint32_t evw) { sink.hit(s, pv, pw, evw); });
+        }
+    }
+    sink.finish();
+}
+
+// Out-lists longer than kWarpMaxDeg: collect them for the CTA kernel.
+static __global__ void wedge_collect_long_kernel(const uint32_t* __restrict__ offsets, uint32_t V,
+                                          uint32_t* __restrict__ list, uint32_t* __restrict__ count) {
+    for (uint64_t u = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u < V;
+         u += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        if (offsets[u + 1] - offsets[u] > kWarpMaxDeg) list[atomicAdd(count, 1u)] = static_cast<uint32_t>(u);
+    }
+}
+
+// CTA per long out-list, handed out dynamically: a shared hash table when the
+// list has at most kCtaMaxDeg entries, otherwise binary search of the list in
+// global memory.
+template <class Sink>
+__global__ void __launch_bounds__(kWedgeThreads) wedge_cta_kernel(const uint32_t* __restrict__ offsets,
+                                                                  const uint32_t* __restrict__ targets,
+                                                                  const uint32_t* __restrict__ long_list,
+                                                                  const uint32_t* __restrict__ long_count,
+                                                                  uint32_t* __restrict__ next_item, Sink sink) {
+    constexpr bool kPos = Sink::kNeedsPos;
+    __shared__ uint32_t s_keys[kCtaSlots];
+    __shared__ uint32_t s_pos[kPos ? kCtaSlots : 1];
+    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_start[kWedgeWarps][32];
+    __shared__ uint32_t s_item;
+    const unsigned warp = threadIdx.x >> 5;
+    const uint32_t n = *long_count;
+    uint32_t* pos = kPos ? s_pos : nullptr;
+    while (true) {
+        if (threadIdx.x == 0) s_item = atomicAdd(next_item, 1u);
+        __syncthreads();
+        const uint32_t h = s_item;
+        if (h >= n) break;
+        const uint32_t u = long_list[h];
+        const uint32_t s = offsets[u], du = offsets[u + 1] - s;
+        const uint32_t* list = targets + s;
+        const bool use_table = du <= kCtaMaxDeg;
+        const uint32_t bits = use_table ? table_bits(du) : 0;
+        if (use_table) {
+            for (uint32_t k = threadIdx.x; k < (1u << bits); k += kWedgeThreads) s_keys[k] = kEmptyKey;
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < du; k += kWedgeThreads) hash_insert<kPos>(s_keys, pos, bits, list[k], k);
+            __syncthreads();
+        }
+        for (uint32_t c = warp * 32; c < du; c += kWedgeThreads)
+            wedge_chunk(
+                offsets, targets, list, du, c, s_excl[warp], s_start[warp],
+                [&](uint32_t w) {
+                    return use_table ? hash_find<kPos>(s_keys, pos, bits, w) : sorted_find(list, du, w);
+                },
+                [&](uint32_t pv, uint32_t pw, uint32_t evw) { sink.hit(s, pv, pw, evw); });
+        __syncthreads();  // the table and s_item are reused by the next list
+    }
+    sink.finish();
+}
+
+// Runs both wedge kernels over a DAG CSR: long out-lists by CTAs first (they
+// hold the heaviest work), then everything else by warps.
+template <class Sink>
+Error run_wedges(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets, uint32_t V, uint32_t min_deg,
+                 Sink sink, const char* tag) {
+    (void)tag;
+    // scratch: [0] next vertex, [1] long-list count, [2] next long list, then the long lists
+    DeviceBuffer<uint32_t> scratch;
+    GCU_TRY(scratch.allocate(dev, 4 + static_cast<uint64_t>(V)));
+    GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, 4 * sizeof(uint32_t), dev.stream), "memset");
+    const unsigned grid = static_cast<unsigned>(dev.sm_count) * 8;
+    const unsigned collect_blocks =
+        static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), static_cast<uint64_t>(dev.sm_count) * 8));
+    GCU_LAUNCH(dev, "wedge_collect_long", wedge_collect_long_kernel, collect_blocks, 256, 0, d_offsets, V,
+               scratch.ptr + 4, scratch.ptr + 1);
+    GCU_LAUNCH(dev, "wedge_cta", wedge_cta_kernel<Sink>, grid, kWedgeThreads, 0, d_offsets, d_targets,
+               scratch.ptr + 4, scratch.ptr + 1, scratch.ptr + 2, sink);
+    GCU_LAUNCH(dev, "wedge_warp", wedge_warp_kernel<Sink>, grid, kWedgeThreads, 0, d_offsets, d_targets, V, min_deg,
+               scratch.ptr, sink);
+    return ok();
+}
+
+}  // namespace gcu

@@ -231,6 +231,24 @@ def test_non_symmetric_csr_follows_reference_formulas(device):
             assert edge_set(r["edges"]) == edge_set(ref["edges"]) and r["iterations"] == ref["iterations"]
 
 
+def test_k_truss_with_self_loops_matches_oracle(device):
+    """Self-loops inflate first-round support in the reference (k_truss.cu:59-92);
+    the incremental peel must reproduce the edges and the round count."""
+    base = G.generate_rmat(12, 8, 0.57, 0.19, 0.19, seed=9)
+    rng = np.random.default_rng(9)
+    src = np.repeat(np.arange(base.num_nodes, dtype=np.uint32), np.diff(base.offsets))
+    pairs = np.stack([src, base.targets], axis=1)
+    loops = rng.choice(base.num_nodes, size=base.num_nodes // 10, replace=False).astype(np.uint32)
+    pairs = np.concatenate([pairs, np.stack([loops, loops], axis=1)])
+    csr = G.from_edge_pairs(pairs, base.num_nodes, True)
+    g = G.GpuGraph.from_csr_arrays(csr, device)
+    for k in (3, 4, 5, 7):
+        r = g.k_truss_array(k)
+        ref = O.k_truss(csr.offsets, csr.targets, k)
+        assert np.array_equal(r["edges"], ref["edges"]), k
+        assert r["iterations"] == ref["iterations"], k
+
+
 def compare_with_oracle(device, csr, sources, pr_iterations, ks, label):
     o, t = csr.offsets, csr.targets
     g = G.GpuGraph.from_csr_arrays(csr, device)
