@@ -1,32 +1,38 @@
-// PageRank: pull SpMV over the CSR with the update, the L1 residual and the
-// dangling mass fused into its epilogue.
+// PageRank: pull SpMV over a degree-relabelled copy of the CSR, with the rank
+// update, the L1 residual and the dangling mass fused into its epilogue.
 //
 // Reference: crates/grafeo-cuda-algos/src/pagerank.rs:46-199 and
 // kernels/pagerank.cu:19-134. Per iteration the reference launches four
 // kernels (dangling sum, thread-per-row SpMV, L1 diff, plus memsets), reads
 // `ranks_in[u] / deg[u]` with two random gathers and a divide per edge, and
-// syncs the host to read the f32 diff. Here:
+// syncs the host to read the f32 diff. What bounds a pull SpMV on a power-law
+// graph is the random gather of the source contributions (one L1TEX sector
+// per edge), not the streamed CSR; the design follows from that:
 //
-//  * Work split: merge-path over (row ends, nonzeros) (Merrill & Garland,
-//    SC'16). Every tile of kTile merge items gets the same amount of work no
-//    matter how skewed the degrees are, so a 160k-degree R-MAT hub is spread
-//    over ~80 tiles instead of one thread.
-//  * Each tile stages its slice of `offsets` and the gathered contributions
-//    c[u] = rank[u] / deg(u) of its nonzeros in shared memory with coalesced
-//    loads; `targets` is streamed once (no L1 allocation), `c` (4V bytes) stays
-//    resident in L2.
-//  * Row sums: FP32 Kahan sums inside each thread; partial sums that cross
-//    threads, tiles or rows are carried in FP64 and combined by a block-wide
-//    segmented scan, then across tiles by a fix-up pass in a fixed order.
-//  * Epilogue per row v: r'[v] = (1-d)/N + d (sum + dangling/N); |r' - r| and
-//    the dangling mass of r' go to FP64 per-tile partials, reduced in a fixed
-//    order by the last block of the fix-up pass (deterministic, no float
-//    atomics); c'[v] = r'[v] / deg(v) is written for the next iteration.
+//  * Relabelling (once per graph, cached): vertices are stably partitioned by
+//    degree class, class c holding degrees in [2^(c-1), 2^c), highest class
+//    first and ids ascending inside a class. Hubs get the smallest new ids,
+//    so their contributions share sectors and cache lines and most gathers
+//    hit L1/L2 lines that are already hot. The relabelled CSR keeps every
+//    list in its original order, so each row's summation order is the
+//    original one.
+//  * Rows of one class have similar length, so each class gets a fixed group
+//    of 2^(c-1) lanes per row (1 to 32): consecutive groups read consecutive
+//    rows (coalesced), no search, no staging, no carries. Rows of 4096 or more
+//    entries are split into 4096-entry segments, one block each, and their
+//    partial sums are added in segment order by the finishing kernel.
+//  * Row sums: FP32 Kahan sums per lane, FP64 across lanes (shuffle tree) and
+//    across segments. Epilogue per row v: r'[v] = (1-d)/N + d (sum +
+//    dangling/N); |r' - r| and the dangling mass of r' go to FP64 per-block
+//    partials that the last block of the finishing kernel reduces in a fixed
+//    order (deterministic, no float atomics); c'[v] = r'[v] / deg(v) is
+//    written for the next iteration.
 //  * The iteration loop stays on the device: each kernel reads a `done` flag
-//    first, so the host can queue iterations ahead and poll the flag once per
+//    first, so the host queues iterations ahead and polls the flag once per
 //    chunk instead of syncing every iteration.
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "device_common.cuh"
 #include "gcu_internal.h"
@@ -34,14 +40,28 @@
 namespace gcu {
 
 constexpr int kPrThreads = 256;
-constexpr int kPrItems = 8;                       // merge items per thread
-constexpr int kPrTile = kPrThreads * kPrItems;    // merge items per tile
-constexpr uint32_t kNoRow = 0xFFFFFFFFu;
+constexpr int kDegClasses = 33;       // class 0: degree 0; class c: degree in [2^(c-1), 2^c)
+constexpr int kLongClass = 13;        // degree >= 4096
+constexpr uint32_t kSegment = 4096;   // entries per long-row segment (one block)
+constexpr int kClassBlock = 1024;     // vertices per block of the class partition
+constexpr int kMaxPhases = 16;
+constexpr int kSmallRows = 4;         // rows per group for classes with fewer than 32 lanes per row
 
-// Shared-memory index with one padding word per 32: each thread walks
-// kPrItems consecutive staged items, so without padding the lanes of a warp
-// would hit every 8th bank (an 8-way conflict on every merge step).
-__device__ __forceinline__ uint32_t pad(uint32_t k) { return k + (k >> 5); }
+enum : uint32_t { kPhaseLong = 0, kPhaseGroup = 1, kPhaseEmpty = 2 };
+
+struct PrPhase {
+    uint32_t first_block;  // first block of this phase
+    uint32_t row_begin, row_end;
+    uint32_t kind;
+    uint32_t log2g;        // lanes per row = 1 << log2g (group phases)
+    uint32_t rows_per_group;
+};
+
+struct PrSchedule {
+    uint32_t nphases;
+    uint32_t total_blocks;
+    PrPhase phase[kMaxPhases];
+};
 
 struct PrState {
     double dangling;   // sum of ranks of dangling vertices in the current input ranks
@@ -53,20 +73,24 @@ struct PrState {
 };
 
 struct PageRankPlan {
-    uint64_t num_tiles = 0;
-    DeviceBuffer<uint2> coords;        // merge-path coordinates (row, nonzero) per tile start
-    DeviceBuffer<float> ranks;         // 2 * V: ping-pong
-    DeviceBuffer<float> contrib;       // 2 * V: ping-pong
-    DeviceBuffer<uint32_t> head_row;   // per tile: row finished here but started in an earlier tile
-    DeviceBuffer<double> head_val;
-    DeviceBuffer<uint32_t> carry_row;  // per tile: row still open at the tile end
-    DeviceBuffer<double> carry_val;
-    DeviceBuffer<double> tile_diff;
-    DeviceBuffer<double> tile_dangle;
-    DeviceBuffer<double> block_partials;  // 2 * fix-up blocks
+    uint32_t long_rows = 0;   // rows [0, long_rows) of the relabelled CSR have >= 4096 entries
+    uint32_t empty_rows = 0;  // rows without entries (the last class)
+    uint32_t fin_blocks = 1;
+    PrSchedule sched{};
+    DeviceBuffer<uint32_t> perm;       // new id -> original id
+    DeviceBuffer<uint32_t> inv;        // original id -> new id
+    DeviceBuffer<uint32_t> poff;       // relabelled offsets (V + 1)
+    DeviceBuffer<uint32_t> ptgt;       // relabelled targets (E)
+    DeviceBuffer<uint2> units;         // long-row segments: (row, segment)
+    DeviceBuffer<uint32_t> unit_begin; // long row i owns units [unit_begin[i], unit_begin[i+1])
+    DeviceBuffer<double> seg_partial;  // one partial sum per unit
+    DeviceBuffer<float> ranks;         // 2 * V: ping-pong, relabelled order
+    DeviceBuffer<float> contrib;       // 2 * V: ping-pong, relabelled order
+    DeviceBuffer<float> ranks_out;     // V: result in original order
+    DeviceBuffer<double> row_partials; // 2 per block of the row kernel
+    DeviceBuffer<double> fin_partials; // 2 per block of the finishing kernel
     DeviceBuffer<PrState> state;
     PrState* host_state = nullptr;     // pinned
-    uint32_t final_buffer = 0;         // which half of `ranks` holds the last result
 };
 
 void destroy_pagerank_plan(PageRankPlan* p) {
@@ -75,274 +99,314 @@ void destroy_pagerank_plan(PageRankPlan* p) {
     delete p;
 }
 
-// ---------------------------------------------------------------- kernels
+// ---------------------------------------------------------------- relabelling kernels
 
-// Merge-path search: coordinate (rows finished, nonzeros consumed) of
-// `diagonal` in the merge of row ends offsets[1..V] with nonzero indices 0..E-1.
-__device__ __forceinline__ uint2 merge_path_search(const uint32_t* __restrict__ offsets, uint32_t V, uint32_t E,
-                                                   uint64_t diagonal) {
-    uint64_t lo = diagonal > E ? diagonal - E : 0;
-    uint64_t hi = diagonal < V ? diagonal : V;
-    while (lo < hi) {
-        uint64_t pivot = (lo + hi) >> 1;
-        // Row end `pivot` comes before nonzero (diagonal - pivot - 1)?
-        if (static_cast<uint64_t>(offsets[pivot + 1]) <= diagonal - pivot - 1)
-            lo = pivot + 1;
-        else
-            hi = pivot;
+__host__ __device__ __forceinline__ uint32_t degree_class(uint32_t d) {
+#ifdef __CUDA_ARCH__
+    return d == 0 ? 0u : 32u - static_cast<uint32_t>(__clz(d));
+#else
+    uint32_t c = 0;
+    while (d) {
+        ++c;
+        d >>= 1;
     }
-    return make_uint2(static_cast<uint32_t>(lo), static_cast<uint32_t>(diagonal - lo));
+    return c;
+#endif
 }
 
-__global__ void pr_plan_kernel(const uint32_t* __restrict__ offsets, uint32_t V, uint32_t E, uint64_t num_tiles,
-                               uint2* __restrict__ coords) {
-    uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t > num_tiles) return;
-    uint64_t total = static_cast<uint64_t>(V) + E;
-    uint64_t diag = std::min<uint64_t>(t * kPrTile, total);
-    coords[t] = merge_path_search(offsets, V, E, diag);
+// counts[(K-1-c) * nblk + blk] = vertices of class c in block blk, so that an
+// exclusive scan gives every (class, block) its first new id, classes descending.
+__global__ void __launch_bounds__(kClassBlock) pr_class_count_kernel(const uint32_t* __restrict__ offsets, uint32_t V,
+                                                                     uint32_t nblk, uint32_t* __restrict__ counts) {
+    __shared__ uint32_t h[kDegClasses];
+    if (threadIdx.x < kDegClasses) h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint64_t v = static_cast<uint64_t>(blockIdx.x) * kClassBlock + threadIdx.x;
+    if (v < V) atomicAdd(&h[degree_class(offsets[v + 1] - offsets[v])], 1u);
+    __syncthreads();
+    if (threadIdx.x < kDegClasses) counts[(kDegClasses - 1 - threadIdx.x) * nblk + blockIdx.x] = h[threadIdx.x];
 }
 
-__global__ void __launch_bounds__(kPrThreads) pr_init_kernel(const uint32_t* __restrict__ offsets, uint32_t V,
-                                                             float r0, float* __restrict__ ranks,
-                                                             float* __restrict__ contrib,
-                                                             double* __restrict__ block_partials) {
-    __shared__ double scratch[32];
-    double dangle = 0.0;
+// Stable scatter: the rank of v among the vertices of its class in its block
+// comes from per-warp class matches and a prefix over the warps.
+__global__ void __launch_bounds__(kClassBlock) pr_class_scatter_kernel(const uint32_t* __restrict__ offsets, uint32_t V,
+                                                                       uint32_t nblk, const uint32_t* __restrict__ cpos,
+                                                                       uint32_t* __restrict__ perm,
+                                                                       uint32_t* __restrict__ inv) {
+    __shared__ uint32_t wcnt[kClassBlock / 32][kDegClasses];
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    for (uint32_t k = threadIdx.x; k < (kClassBlock / 32) * kDegClasses; k += kClassBlock) (&wcnt[0][0])[k] = 0;
+    __syncthreads();
+    const uint64_t v = static_cast<uint64_t>(blockIdx.x) * kClassBlock + threadIdx.x;
+    const uint32_t c = v < V ? degree_class(offsets[v + 1] - offsets[v]) : kDegClasses;
+    const unsigned same = __match_any_sync(kFullMask, c);
+    const uint32_t rank = __popc(same & ((1u << lane) - 1));
+    if (c < kDegClasses && lane == static_cast<unsigned>(__ffs(same) - 1)) wcnt[warp][c] = __popc(same);
+    __syncthreads();
+    if (threadIdx.x < kDegClasses) {
+        uint32_t run = 0;
+        for (int w = 0; w < kClassBlock / 32; ++w) {
+            const uint32_t t = wcnt[w][threadIdx.x];
+            wcnt[w][threadIdx.x] = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+    if (v < V) {
+        const uint32_t pos = cpos[(kDegClasses - 1 - c) * nblk + blockIdx.x] + wcnt[warp][c] + rank;
+        perm[pos] = static_cast<uint32_t>(v);
+        inv[v] = pos;
+    }
+}
+
+// First new id of every class (index c), plus V at index K.
+__global__ void pr_class_starts_kernel(const uint32_t* __restrict__ cpos, uint32_t nblk, uint32_t* __restrict__ starts) {
+    const uint32_t c = threadIdx.x;
+    if (c < kDegClasses) starts[c] = cpos[(kDegClasses - 1 - c) * nblk];
+    if (c == kDegClasses) starts[c] = cpos[kDegClasses * nblk];
+}
+
+__global__ void pr_perm_degree_kernel(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ perm,
+                                      uint32_t V, uint32_t* __restrict__ pdeg) {
+    for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < V;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t u = perm[r];
+        pdeg[r] = offsets[u + 1] - offsets[u];
+    }
+}
+
+// Relabelled row r = original row perm[r] with every target renamed; a warp
+// walks 32 rows, the lanes stride over each row.
+__global__ void __launch_bounds__(256) pr_perm_fill_kernel(const uint32_t* __restrict__ offsets,
+                                                           const uint32_t* __restrict__ targets,
+                                                           const uint32_t* __restrict__ perm,
+                                                           const uint32_t* __restrict__ inv,
+                                                           const uint32_t* __restrict__ poff, uint32_t V,
+                                                           uint32_t* __restrict__ ptgt) {
+    const unsigned lane = lane_id();
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
+        const uint32_t count = static_cast<uint32_t>(min_u64(32, V - base));
+        uint32_t s = 0, e = 0, o = 0;
+        if (lane < count) {
+            const uint32_t u = perm[base + lane];
+            s = offsets[u];
+            e = offsets[u + 1];
+            o = poff[base + lane];
+        }
+        for (uint32_t i = 0; i < count; ++i) {
+            const uint32_t start = __shfl_sync(kFullMask, s, i), end = __shfl_sync(kFullMask, e, i);
+            const uint32_t out = __shfl_sync(kFullMask, o, i);
+            for (uint32_t j = start + lane; j < end; j += 32) ptgt[out + (j - start)] = inv[ld_stream(targets + j)];
+        }
+    }
+}
+
+__global__ void pr_init_kernel(const uint32_t* __restrict__ poff, uint32_t V, float r0, float* __restrict__ ranks,
+                               float* __restrict__ contrib) {
     for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
          v += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        uint32_t deg = offsets[v + 1] - offsets[v];
+        const uint32_t deg = poff[v + 1] - poff[v];
         ranks[v] = r0;
         contrib[v] = deg > 0 ? r0 / static_cast<float>(deg) : 0.f;
-        if (deg == 0) dangle += static_cast<double>(r0);
-    }
-    dangle = block_sum(dangle, scratch);
-    if (threadIdx.x == 0) block_partials[blockIdx.x] = dangle;
-}
-
-__global__ void __launch_bounds__(1024) pr_init_reduce_kernel(const double* __restrict__ block_partials,
-                                                              uint32_t nblocks, PrState* __restrict__ state) {
-    __shared__ double scratch[32];
-    double s = 0.0;
-    for (uint32_t i = threadIdx.x; i < nblocks; i += blockDim.x) s += block_partials[i];
-    s = block_sum(s, scratch);
-    if (threadIdx.x == 0) {
-        state->dangling = s;
-        state->last_diff = INFINITY;
-        state->iterations = 0;
-        state->done = 0;
-        state->ticket = 0;
     }
 }
 
-// Row update shared by the tile and fix-up kernels.
+__global__ void pr_unpermute_kernel(const float* __restrict__ ranks, const uint32_t* __restrict__ inv, uint32_t V,
+                                    float* __restrict__ out) {
+    for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
+         v += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        out[v] = ranks[inv[v]];
+    }
+}
+
+// ---------------------------------------------------------------- iteration kernels
+
+// Row update shared by the row and finishing kernels.
 __device__ __forceinline__ void pr_finish_row(uint32_t v, double sum, uint32_t deg, const float* __restrict__ rank_in,
                                               float* __restrict__ rank_out, float* __restrict__ contrib_out,
                                               double base, double damp, double spread, double& diff,
                                               double& dangle) {
-    float r = static_cast<float>(base + damp * (sum + spread));
-    float old = rank_in[v];
+    const float r = static_cast<float>(base + damp * (sum + spread));
+    const float old = rank_in[v];
     diff += fabs(static_cast<double>(r) - static_cast<double>(old));
     rank_out[v] = r;
     contrib_out[v] = deg > 0 ? r / static_cast<float>(deg) : 0.f;
     if (deg == 0) dangle += static_cast<double>(r);
 }
 
-__global__ void __launch_bounds__(kPrThreads) pr_tile_kernel(
-    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, const uint2* __restrict__ coords,
-    const float* __restrict__ rank_in, const float* __restrict__ contrib_in, float* __restrict__ rank_out,
-    float* __restrict__ contrib_out, uint32_t V, double base, double damp, const PrState* __restrict__ state,
-    uint32_t* __restrict__ head_row, double* __restrict__ head_val, uint32_t* __restrict__ carry_row,
-    double* __restrict__ carry_val, double* __restrict__ tile_diff, double* __restrict__ tile_dangle) {
+__device__ __forceinline__ void kahan_add(float& acc, float& comp, float x) {
+    const float y = x - comp;
+    const float t = acc + y;
+    comp = (t - acc) - y;
+    acc = t;
+}
+
+// Sum over lanes of an aligned group of 2^log2g lanes (all 32 lanes call it).
+__device__ __forceinline__ double group_sum(double v, uint32_t log2g) {
+    for (uint32_t o = (1u << log2g) >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(kFullMask, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(kPrThreads) pr_rows_kernel(
+    const uint32_t* __restrict__ poff, const uint32_t* __restrict__ ptgt, const float* __restrict__ rank_in,
+    const float* __restrict__ contrib_in, float* __restrict__ rank_out, float* __restrict__ contrib_out, uint32_t V,
+    double base, double damp, const PrState* __restrict__ state, const PrSchedule sched,
+    const uint2* __restrict__ units, double* __restrict__ seg_partial, double* __restrict__ row_partials) {
     if (state->done) return;
-    __shared__ uint32_t s_off[kPrTile + 2 + (kPrTile + 2) / 32 + 1];
-    __shared__ float s_val[kPrTile + kPrTile / 32];
-    __shared__ double s_warp_v[kPrThreads / 32];
-    __shared__ int s_warp_f[kPrThreads / 32];
-    __shared__ uint32_t s_defer_row;
-    __shared__ double s_defer_val;
     __shared__ double scratch[32];
-
-    const uint32_t t = blockIdx.x;
-    const uint2 c0 = coords[t], c1 = coords[t + 1];
-    const uint32_t r0 = c0.x, z0 = c0.y;
-    const uint32_t nrows = c1.x - c0.x, nnz = c1.y - c0.y;
-    const uint32_t items = nrows + nnz;
+    const uint32_t b = blockIdx.x;
+    uint32_t pi = 0;
+    while (pi + 1 < sched.nphases && sched.phase[pi + 1].first_block <= b) ++pi;
+    const PrPhase ph = sched.phase[pi];
     const double spread = state->dangling / static_cast<double>(V);
-
-    // Stage offsets[r0 .. r0 + nrows + 1] and the gathered contributions.
-    for (uint32_t k = threadIdx.x; k < nrows + 2; k += kPrThreads) {
-        uint64_t r = static_cast<uint64_t>(r0) + k;
-        s_off[pad(k)] = r <= V ? ld_stream(offsets + r) : 0xFFFFFFFFu;
-    }
-    {
-        // All of this thread's target loads first, then all gathers, so every
-        // thread keeps kPrItems independent requests in flight.
-        uint32_t u[kPrItems];
-#pragma unroll
-        for (int q = 0; q < kPrItems; ++q) {
-            const uint32_t k = threadIdx.x + q * kPrThreads;
-            u[q] = k < nnz ? ld_stream(targets + z0 + k) : 0u;
-        }
-#pragma unroll
-        for (int q = 0; q < kPrItems; ++q) {
-            const uint32_t k = threadIdx.x + q * kPrThreads;
-            if (k < nnz) s_val[pad(k)] = __ldg(contrib_in + u[q]);
-        }
-    }
-    if (threadIdx.x == 0) s_defer_row = kNoRow;
-    __syncthreads();
-
-    // This thread's start on the merge path inside the tile.
-    const uint32_t dk = min(static_cast<uint32_t>(threadIdx.x) * kPrItems, items);
-    uint32_t lo = dk > nnz ? dk - nnz : 0, hi = min(dk, nrows);
-    while (lo < hi) {
-        uint32_t p = (lo + hi) >> 1;
-        if (s_off[pad(p + 1)] <= z0 + dk - p - 1)
-            lo = p + 1;
-        else
-            hi = p;
-    }
-    uint32_t rr = lo, jj = dk - lo;
-    const uint32_t stop = min(dk + kPrItems, items);
-
-    float acc = 0.f, comp = 0.f;  // Kahan sum of the open row
-    bool has_head = false;
-    double head_partial = 0.0;
-    uint32_t head_local = 0;
     double my_diff = 0.0, my_dangle = 0.0;
+
+    if (ph.kind == kPhaseLong) {
+        // One segment of a long row: 16 entries per thread, 4 loads in flight.
+        const uint2 unit = units[b - ph.first_block];
+        const uint32_t row_start = poff[unit.x], row_end = poff[unit.x + 1];
+        const uint32_t s0 = row_start + unit.y * kSegment;
+        const uint32_t s1 = min(s0 + kSegment, row_end);
+        float acc = 0.f, comp = 0.f;
+        uint32_t j = s0 + threadIdx.x;
+        for (; j + 3 * kPrThreads < s1; j += 4 * kPrThreads) {
+            const uint32_t t0 = ld_stream(ptgt + j), t1 = ld_stream(ptgt + j + kPrThreads);
+            const uint32_t t2 = ld_stream(ptgt + j + 2 * kPrThreads), t3 = ld_stream(ptgt + j + 3 * kPrThreads);
+            const float c0 = __ldg(contrib_in + t0), c1 = __ldg(contrib_in + t1);
+            const float c2 = __ldg(contrib_in + t2), c3 = __ldg(contrib_in + t3);
+            kahan_add(acc, comp, c0);
+            kahan_add(acc, comp, c1);
+            kahan_add(acc, comp, c2);
+            kahan_add(acc, comp, c3);
+        }
+        for (; j < s1; j += kPrThreads) kahan_add(acc, comp, __ldg(contrib_in + ld_stream(ptgt + j)));
+        const double part = block_sum(static_cast<double>(acc) - static_cast<double>(comp), scratch);
+        if (threadIdx.x == 0) seg_partial[b - ph.first_block] = part;
+    } else if (ph.kind == kPhaseGroup) {
+        const uint32_t log2g = ph.log2g, g = 1u << log2g;
+        const uint32_t groups = kPrThreads >> log2g;
+        const uint32_t group = threadIdx.x >> log2g, lig = threadIdx.x & (g - 1);
+        const uint32_t first = ph.row_begin + (b - ph.first_block) * groups * ph.rows_per_group;
+        if (g < 32) {
+            // Rows shorter than 2g: at most two entries per lane and row, all
+            // kSmallRows rows loaded before any is summed.
+            uint32_t rs[kSmallRows], re[kSmallRows], t[kSmallRows][2];
 #pragma unroll
-    for (int q = 0; q < kPrItems; ++q) {
-        if (dk + q >= stop) break;
-        if (jj < nnz && z0 + jj < s_off[pad(rr + 1)]) {
-            float y = s_val[pad(jj)] - comp;
-            float s = acc + y;
-            comp = (s - acc) - y;
-            acc = s;
-            ++jj;
-        } else {
-            double sum = static_cast<double>(acc) - static_cast<double>(comp);
-            if (!has_head) {
-                has_head = true;
-                head_partial = sum;
-                head_local = rr;
-            } else {
-                pr_finish_row(r0 + rr, sum, s_off[pad(rr + 1)] - s_off[pad(rr)], rank_in, rank_out, contrib_out, base, damp,
-                              spread, my_diff, my_dangle);
+            for (int s = 0; s < kSmallRows; ++s) {
+                const uint32_t row = first + s * groups + group;
+                rs[s] = 0;
+                re[s] = 0;
+                if (row < ph.row_end) {
+                    rs[s] = poff[row];
+                    re[s] = poff[row + 1];
+                }
             }
-            acc = 0.f;
-            comp = 0.f;
-            ++rr;
-        }
-    }
-
-    // Block-wide segmented scan of the carries: a thread that finished a row
-    // starts a new segment. The exclusive value is what earlier threads add to
-    // this thread's first finished row.
-    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
-    double v = static_cast<double>(acc) - static_cast<double>(comp);
-    int f = has_head ? 1 : 0;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        double pv = __shfl_up_sync(kFullMask, v, o);
-        int pf = __shfl_up_sync(kFullMask, f, o);
-        if (lane >= static_cast<unsigned>(o)) {
-            if (!f) v += pv;
-            f |= pf;
-        }
-    }
-    if (lane == 31) {
-        s_warp_v[warp] = v;
-        s_warp_f[warp] = f;
-    }
-    __syncthreads();
-    double pre_v = 0.0;
-    int pre_f = 0;
-    for (unsigned w = 0; w < warp; ++w) {
-        if (s_warp_f[w]) {
-            pre_v = s_warp_v[w];
-            pre_f = 1;
+            for (int s = 0; s < kSmallRows; ++s) {
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const uint32_t j = rs[s] + lig + k * g;
+                    t[s][k] = j < re[s] ? ld_stream(ptgt + j) : 0xFFFFFFFFu;
+                }
+            }
+            float c[kSmallRows][2];
+#pragma unroll
+            for (int s = 0; s < kSmallRows; ++s) {
+#pragma unroll
+                for (int k = 0; k < 2; ++k) c[s][k] = t[s][k] != 0xFFFFFFFFu ? __ldg(contrib_in + t[s][k]) : 0.f;
+            }
+#pragma unroll
+            for (int s = 0; s < kSmallRows; ++s) {
+                const uint32_t row = first + s * groups + group;
+                double v = static_cast<double>(c[s][0]) + static_cast<double>(c[s][1]);
+                v = group_sum(v, log2g);
+                if (lig == 0 && row < ph.row_end)
+                    pr_finish_row(row, v, re[s] - rs[s], rank_in, rank_out, contrib_out, base, damp, spread, my_diff,
+                                  my_dangle);
+            }
         } else {
-            pre_v += s_warp_v[w];
+            // A warp per row (32 to 4095 entries), 4 loads in flight per lane.
+            for (uint32_t s = 0; s < ph.rows_per_group; ++s) {
+                const uint32_t row = first + s * groups + group;
+                float acc = 0.f, comp = 0.f;
+                uint32_t rs = 0, re = 0;
+                if (row < ph.row_end) {
+                    rs = poff[row];
+                    re = poff[row + 1];
+                }
+                uint32_t j = rs + lig;
+                for (; j + 96 < re; j += 128) {
+                    const uint32_t t0 = ld_stream(ptgt + j), t1 = ld_stream(ptgt + j + 32);
+                    const uint32_t t2 = ld_stream(ptgt + j + 64), t3 = ld_stream(ptgt + j + 96);
+                    const float c0 = __ldg(contrib_in + t0), c1 = __ldg(contrib_in + t1);
+                    const float c2 = __ldg(contrib_in + t2), c3 = __ldg(contrib_in + t3);
+                    kahan_add(acc, comp, c0);
+                    kahan_add(acc, comp, c1);
+                    kahan_add(acc, comp, c2);
+                    kahan_add(acc, comp, c3);
+                }
+                for (; j < re; j += 32) kahan_add(acc, comp, __ldg(contrib_in + ld_stream(ptgt + j)));
+                const double v = group_sum(static_cast<double>(acc) - static_cast<double>(comp), 5);
+                if (lig == 0 && row < ph.row_end)
+                    pr_finish_row(row, v, re - rs, rank_in, rank_out, contrib_out, base, damp, spread, my_diff,
+                                  my_dangle);
+            }
         }
-    }
-    if (!f) v += pre_v;
-    f |= pre_f;
-    double ex_v = __shfl_up_sync(kFullMask, v, 1);
-    int ex_f = __shfl_up_sync(kFullMask, f, 1);
-    if (lane == 0) {
-        ex_v = pre_v;
-        ex_f = pre_f;
-    }
-
-    if (has_head) {
-        double total = head_partial + ex_v;
-        uint32_t row = r0 + head_local;
-        // The tile's first row began in an earlier tile: finish it in the fix-up.
-        if (!ex_f && s_off[pad(0)] < z0) {
-            s_defer_row = row;
-            s_defer_val = total;
-        } else {
-            pr_finish_row(row, total, s_off[pad(head_local + 1)] - s_off[pad(head_local)], rank_in, rank_out, contrib_out,
-                          base, damp, spread, my_diff, my_dangle);
-        }
-    }
-    if (threadIdx.x == kPrThreads - 1) {
-        carry_row[t] = c1.x;
-        carry_val[t] = v;
+    } else {
+        // Rows without entries: the teleport and dangling share only.
+        const uint32_t row = ph.row_begin + (b - ph.first_block) * kPrThreads + threadIdx.x;
+        if (row < ph.row_end)
+            pr_finish_row(row, 0.0, 0, rank_in, rank_out, contrib_out, base, damp, spread, my_diff, my_dangle);
     }
     my_diff = block_sum(my_diff, scratch);
     my_dangle = block_sum(my_dangle, scratch);
     if (threadIdx.x == 0) {
-        tile_diff[t] = my_diff;
-        tile_dangle[t] = my_dangle;
-        head_row[t] = s_defer_row;
-        head_val[t] = s_defer_val;
+        row_partials[2 * b] = my_diff;
+        row_partials[2 * b + 1] = my_dangle;
     }
 }
 
-// Finishes rows that span tiles, then the last block reduces the per-tile and
-// per-block partials in a fixed order and advances the iteration state.
-__global__ void __launch_bounds__(256) pr_fixup_kernel(
-    const uint32_t* __restrict__ offsets, uint64_t num_tiles, const float* __restrict__ rank_in,
-    float* __restrict__ rank_out, float* __restrict__ contrib_out, uint32_t V, double base, double damp,
-    PrState* __restrict__ state, double tolerance, const uint32_t* __restrict__ head_row,
-    const double* __restrict__ head_val, const uint32_t* __restrict__ carry_row,
-    const double* __restrict__ carry_val, const double* __restrict__ tile_diff,
-    const double* __restrict__ tile_dangle, double* __restrict__ block_partials) {
+// Finishes the long rows from their segment partials (in segment order), then
+// the last block reduces all partials in a fixed order and advances the state.
+__global__ void __launch_bounds__(256) pr_finish_kernel(
+    const uint32_t* __restrict__ poff, uint32_t long_rows, const uint32_t* __restrict__ unit_begin,
+    const double* __restrict__ seg_partial, const float* __restrict__ rank_in, float* __restrict__ rank_out,
+    float* __restrict__ contrib_out, uint32_t V, double base, double damp, PrState* __restrict__ state,
+    double tolerance, const double* __restrict__ row_partials, uint32_t row_blocks,
+    double* __restrict__ fin_partials) {
     if (state->done) return;
     __shared__ double scratch[32];
     __shared__ bool s_last;
     const double spread = state->dangling / static_cast<double>(V);
     double d = 0.0, g = 0.0;
-    uint64_t t = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t < num_tiles) {
-        d = tile_diff[t];
-        g = tile_dangle[t];
-        uint32_t row = head_row[t];
-        if (row != kNoRow) {
-            double sum = head_val[t];
-            for (int64_t s = static_cast<int64_t>(t) - 1; s >= 0 && carry_row[s] == row; --s) sum += carry_val[s];
-            pr_finish_row(row, sum, offsets[row + 1] - offsets[row], rank_in, rank_out, contrib_out, base, damp,
-                          spread, d, g);
-        }
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < long_rows) {
+        double sum = 0.0;
+        for (uint32_t u = unit_begin[i]; u < unit_begin[i + 1]; ++u) sum += seg_partial[u];
+        pr_finish_row(i, sum, poff[i + 1] - poff[i], rank_in, rank_out, contrib_out, base, damp, spread, d, g);
     }
     d = block_sum(d, scratch);
     g = block_sum(g, scratch);
     if (threadIdx.x == 0) {
-        block_partials[2 * blockIdx.x] = d;
-        block_partials[2 * blockIdx.x + 1] = g;
+        fin_partials[2 * blockIdx.x] = d;
+        fin_partials[2 * blockIdx.x + 1] = g;
         __threadfence();
-        unsigned ticket = atomicAdd(&state->ticket, 1u);
+        const unsigned ticket = atomicAdd(&state->ticket, 1u);
         s_last = ticket == gridDim.x - 1;
     }
     __syncthreads();
     if (!s_last) return;
     __threadfence();
     double dd = 0.0, gg = 0.0;
-    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-        dd += __ldcg(block_partials + 2 * b);
-        gg += __ldcg(block_partials + 2 * b + 1);
+    for (uint32_t k = threadIdx.x; k < row_blocks; k += blockDim.x) {
+        dd += __ldcg(row_partials + 2 * k);
+        gg += __ldcg(row_partials + 2 * k + 1);
+    }
+    for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+        dd += __ldcg(fin_partials + 2 * k);
+        gg += __ldcg(fin_partials + 2 * k + 1);
     }
     dd = block_sum(dd, scratch);
     gg = block_sum(gg, scratch);
@@ -361,26 +425,111 @@ static Error ensure_plan(GraphImpl& g) {
     if (g.pr_plan) return ok();
     DeviceImpl& dev = *g.dev;
     auto plan = std::unique_ptr<PageRankPlan, void (*)(PageRankPlan*)>(new PageRankPlan, destroy_pagerank_plan);
+    PageRankPlan& p = *plan;
     const uint32_t V = g.num_nodes, E = g.num_edges;
-    const uint64_t total = static_cast<uint64_t>(V) + E;
-    plan->num_tiles = ceil_div_u64(total, kPrTile);
-    const uint64_t nt = plan->num_tiles;
-    GCU_TRY(plan->coords.allocate(dev, nt + 1));
-    GCU_TRY(plan->ranks.allocate(dev, 2 * static_cast<uint64_t>(V)));
-    GCU_TRY(plan->contrib.allocate(dev, 2 * static_cast<uint64_t>(V)));
-    GCU_TRY(plan->head_row.allocate(dev, nt));
-    GCU_TRY(plan->head_val.allocate(dev, nt));
-    GCU_TRY(plan->carry_row.allocate(dev, nt));
-    GCU_TRY(plan->carry_val.allocate(dev, nt));
-    GCU_TRY(plan->tile_diff.allocate(dev, nt));
-    GCU_TRY(plan->tile_dangle.allocate(dev, nt));
-    uint64_t fix_blocks = ceil_div_u64(nt, 256);
-    uint64_t init_blocks = std::min<uint64_t>(ceil_div_u64(V, kPrThreads), static_cast<uint64_t>(dev.sm_count) * 8);
-    GCU_TRY(plan->block_partials.allocate(dev, 2 * std::max(fix_blocks, init_blocks)));
-    GCU_TRY(plan->state.allocate(dev, 1));
-    GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&plan->host_state), sizeof(PrState)), "cudaMallocHost");
-    GCU_LAUNCH(dev, "pr_plan", pr_plan_kernel, static_cast<unsigned>(ceil_div_u64(nt + 1, 256)), 256, 0,
-               g.offsets.ptr, V, E, nt, plan->coords.ptr);
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned vgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
+
+    // 1. Stable partition of the vertices by degree class, highest first.
+    const uint32_t nblk = static_cast<uint32_t>(ceil_div_u64(V, kClassBlock));
+    const uint64_t ncount = static_cast<uint64_t>(kDegClasses) * nblk;
+    DeviceBuffer<uint32_t> counts, cpos, starts;
+    GCU_TRY(counts.allocate(dev, ncount));
+    GCU_TRY(cpos.allocate(dev, ncount + 1));
+    GCU_TRY(starts.allocate(dev, kDegClasses + 1));
+    GCU_TRY(p.perm.allocate(dev, V));
+    GCU_TRY(p.inv.allocate(dev, V));
+    GCU_LAUNCH(dev, "pr_class_count", pr_class_count_kernel, nblk, kClassBlock, 0, g.offsets.ptr, V, nblk,
+               counts.ptr);
+    GCU_TRY(exclusive_scan_u32(dev, counts.ptr, cpos.ptr, ncount));
+    GCU_LAUNCH(dev, "pr_class_scatter", pr_class_scatter_kernel, nblk, kClassBlock, 0, g.offsets.ptr, V, nblk,
+               cpos.ptr, p.perm.ptr, p.inv.ptr);
+    GCU_LAUNCH(dev, "pr_class_starts", pr_class_starts_kernel, 1, 64, 0, cpos.ptr, nblk, starts.ptr);
+
+    // 2. Relabelled CSR.
+    GCU_TRY(p.poff.allocate(dev, static_cast<uint64_t>(V) + 1));
+    GCU_TRY(p.ptgt.allocate(dev, E));
+    GCU_LAUNCH(dev, "pr_perm_degree", pr_perm_degree_kernel, vgrid, 256, 0, g.offsets.ptr, p.perm.ptr, V, p.poff.ptr);
+    GCU_TRY(exclusive_scan_u32(dev, p.poff.ptr, p.poff.ptr, V));
+    if (E > 0) {
+        GCU_LAUNCH(dev, "pr_perm_fill", pr_perm_fill_kernel, vgrid, 256, 0, g.offsets.ptr, g.targets.ptr, p.perm.ptr,
+                   p.inv.ptr, p.poff.ptr, V, p.ptgt.ptr);
+    }
+    uint32_t cls[kDegClasses + 1];
+    GCU_CUDA(cudaMemcpyAsync(cls, starts.ptr, sizeof(cls), cudaMemcpyDeviceToHost, dev.stream), "copy");
+    GCU_TRY(dev.sync());
+    // Rows of class c (new ids) are [begin[c], end[c]); classes are laid out
+    // from K-1 down to 0, so class c ends where class c-1 begins.
+    std::vector<uint32_t> begin(kDegClasses), end(kDegClasses);
+    for (int c = 0; c < kDegClasses; ++c) {
+        begin[c] = cls[c];
+        end[c] = c == 0 ? V : cls[c - 1];
+    }
+    p.long_rows = begin[kLongClass - 1];  // classes >= kLongClass occupy [0, begin[kLongClass - 1])
+    p.empty_rows = end[0] - begin[0];
+
+    // 3. Long-row segments.
+    std::vector<uint32_t> long_off(p.long_rows + 1, 0);
+    if (p.long_rows > 0) {
+        GCU_CUDA(cudaMemcpyAsync(long_off.data(), p.poff.ptr, sizeof(uint32_t) * (p.long_rows + 1),
+                                 cudaMemcpyDeviceToHost, dev.stream),
+                 "copy");
+        GCU_TRY(dev.sync());
+    }
+    std::vector<uint2> units;
+    std::vector<uint32_t> unit_begin(p.long_rows + 1, 0);
+    for (uint32_t i = 0; i < p.long_rows; ++i) {
+        unit_begin[i] = static_cast<uint32_t>(units.size());
+        const uint32_t deg = long_off[i + 1] - long_off[i];
+        for (uint32_t sgm = 0; sgm * kSegment < deg; ++sgm) units.push_back(make_uint2(i, sgm));
+    }
+    unit_begin[p.long_rows] = static_cast<uint32_t>(units.size());
+    GCU_TRY(p.units.allocate(dev, std::max<size_t>(units.size(), 1)));
+    GCU_TRY(p.unit_begin.allocate(dev, unit_begin.size()));
+    GCU_TRY(p.seg_partial.allocate(dev, std::max<size_t>(units.size(), 1)));
+    if (!units.empty())
+        GCU_CUDA(cudaMemcpyAsync(p.units.ptr, units.data(), sizeof(uint2) * units.size(), cudaMemcpyHostToDevice,
+                                 dev.stream),
+                 "copy");
+    GCU_CUDA(cudaMemcpyAsync(p.unit_begin.ptr, unit_begin.data(), sizeof(uint32_t) * unit_begin.size(),
+                             cudaMemcpyHostToDevice, dev.stream),
+             "copy");
+
+    // 4. Block schedule: long segments, then classes kLongClass-1 .. 1, then empty rows.
+    PrSchedule& s = p.sched;
+    s.nphases = 0;
+    uint32_t blocks = 0;
+    auto add = [&](uint32_t kind, uint32_t rb, uint32_t re, uint32_t log2g, uint32_t rpg, uint32_t nb) {
+        if (nb == 0) return;
+        PrPhase& ph = s.phase[s.nphases++];
+        ph.first_block = blocks;
+        ph.row_begin = rb;
+        ph.row_end = re;
+        ph.kind = kind;
+        ph.log2g = log2g;
+        ph.rows_per_group = rpg;
+        blocks += nb;
+    };
+    add(kPhaseLong, 0, p.long_rows, 0, 0, static_cast<uint32_t>(units.size()));
+    for (int c = kLongClass - 1; c >= 1; --c) {
+        const uint32_t rows = end[c] - begin[c];
+        const uint32_t log2g = std::min<uint32_t>(static_cast<uint32_t>(c - 1), 5);
+        const uint32_t rpg = log2g < 5 ? kSmallRows : 1;
+        const uint32_t per_block = (kPrThreads >> log2g) * rpg;
+        add(kPhaseGroup, begin[c], end[c], log2g, rpg, static_cast<uint32_t>(ceil_div_u64(rows, per_block)));
+    }
+    add(kPhaseEmpty, begin[0], end[0], 0, 0, static_cast<uint32_t>(ceil_div_u64(p.empty_rows, kPrThreads)));
+    s.total_blocks = blocks;
+    p.fin_blocks = static_cast<uint32_t>(std::max<uint64_t>(1, ceil_div_u64(p.long_rows, 256)));
+
+    GCU_TRY(p.ranks.allocate(dev, 2 * static_cast<uint64_t>(V)));
+    GCU_TRY(p.contrib.allocate(dev, 2 * static_cast<uint64_t>(V)));
+    GCU_TRY(p.ranks_out.allocate(dev, V));
+    GCU_TRY(p.row_partials.allocate(dev, 2 * static_cast<uint64_t>(std::max<uint32_t>(blocks, 1))));
+    GCU_TRY(p.fin_partials.allocate(dev, 2 * static_cast<uint64_t>(p.fin_blocks)));
+    GCU_TRY(p.state.allocate(dev, 1));
+    GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p.host_state), sizeof(PrState)), "cudaMallocHost");
+    GCU_TRY(dev.sync());
     g.pr_plan = plan.release();
     return ok();
 }
@@ -397,22 +546,22 @@ Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float toler
     DeviceImpl& dev = *g.dev;
     GCU_TRY(ensure_plan(g));
     PageRankPlan& p = *g.pr_plan;
-    const uint64_t nt = p.num_tiles;
     float* ranks[2] = {p.ranks.ptr, p.ranks.ptr + V};
     float* contrib[2] = {p.contrib.ptr, p.contrib.ptr + V};
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned vgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
 
     const float r0 = 1.0f / static_cast<float>(V);  // pagerank.rs:83
-    const unsigned init_blocks =
-        static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, kPrThreads), static_cast<uint64_t>(dev.sm_count) * 8));
-    GCU_LAUNCH(dev, "pr_init", pr_init_kernel, init_blocks, kPrThreads, 0, g.offsets.ptr, V, r0, ranks[0],
-               contrib[0], p.block_partials.ptr);
-    GCU_LAUNCH(dev, "pr_init_reduce", pr_init_reduce_kernel, 1, 1024, 0, p.block_partials.ptr, init_blocks,
-               p.state.ptr);
+    GCU_LAUNCH(dev, "pr_init", pr_init_kernel, vgrid, 256, 0, p.poff.ptr, V, r0, ranks[0], contrib[0]);
+    PrState init{};
+    init.dangling = static_cast<double>(p.empty_rows) * static_cast<double>(r0);
+    init.last_diff = INFINITY;
+    *p.host_state = init;
+    GCU_CUDA(cudaMemcpyAsync(p.state.ptr, p.host_state, sizeof(PrState), cudaMemcpyHostToDevice, dev.stream), "copy");
 
     const double damp = static_cast<double>(damping);
     const double base = (1.0 - damp) / static_cast<double>(V);
     const double tol = static_cast<double>(tolerance);
-    const unsigned fix_blocks = static_cast<unsigned>(ceil_div_u64(nt, 256));
 
     // Queue iterations in chunks; the device stops itself once converged, so
     // the host only polls the state between chunks.
@@ -423,19 +572,17 @@ Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float toler
     bool stop = false;
     Error err = ok();
     while (launched < max_iterations && !stop) {
-        uint32_t n = std::min(chunk, max_iterations - launched);
+        const uint32_t n = std::min(chunk, max_iterations - launched);
         for (uint32_t i = 0; i < n && err.ok(); ++i) {
             const uint32_t it = launched + i;
             const int in = it & 1, out = in ^ 1;
             err = [&]() -> Error {
-                GCU_LAUNCH(dev, "pr_tile", pr_tile_kernel, static_cast<unsigned>(nt), kPrThreads, 0, g.offsets.ptr,
-                           g.targets.ptr, p.coords.ptr, ranks[in], contrib[in], ranks[out], contrib[out], V, base,
-                           damp, p.state.ptr, p.head_row.ptr, p.head_val.ptr, p.carry_row.ptr, p.carry_val.ptr,
-                           p.tile_diff.ptr, p.tile_dangle.ptr);
-                GCU_LAUNCH(dev, "pr_fixup", pr_fixup_kernel, fix_blocks, 256, 0, g.offsets.ptr, nt, ranks[in],
-                           ranks[out], contrib[out], V, base, damp, p.state.ptr, tol, p.head_row.ptr, p.head_val.ptr,
-                           p.carry_row.ptr, p.carry_val.ptr, p.tile_diff.ptr, p.tile_dangle.ptr,
-                           p.block_partials.ptr);
+                GCU_LAUNCH(dev, "pr_rows", pr_rows_kernel, p.sched.total_blocks, kPrThreads, 0, p.poff.ptr,
+                           p.ptgt.ptr, ranks[in], contrib[in], ranks[out], contrib[out], V, base, damp, p.state.ptr,
+                           p.sched, p.units.ptr, p.seg_partial.ptr, p.row_partials.ptr);
+                GCU_LAUNCH(dev, "pr_finish", pr_finish_kernel, p.fin_blocks, 256, 0, p.poff.ptr, p.long_rows,
+                           p.unit_begin.ptr, p.seg_partial.ptr, ranks[in], ranks[out], contrib[out], V, base, damp,
+                           p.state.ptr, tol, p.row_partials.ptr, p.sched.total_blocks, p.fin_partials.ptr);
                 return ok();
             }();
         }
@@ -454,18 +601,15 @@ Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float toler
     cudaEventDestroy(polled);
     GCU_TRY(err);
     GCU_TRY(dev.sync());
-    if (launched == 0) {
-        p.host_state->iterations = 0;
-        p.host_state->done = 0;
-    }
+    if (launched == 0) *p.host_state = init;
     const uint32_t iters = p.host_state->iterations;
-    p.final_buffer = iters & 1;
+    GCU_LAUNCH(dev, "pr_unpermute", pr_unpermute_kernel, vgrid, 256, 0, ranks[iters & 1], p.inv.ptr, V,
+               p.ranks_out.ptr);
     if (host_ranks) {
-        GCU_CUDA(cudaMemcpyAsync(host_ranks, ranks[p.final_buffer], sizeof(float) * V, cudaMemcpyDeviceToHost,
-                                 dev.stream),
+        GCU_CUDA(cudaMemcpyAsync(host_ranks, p.ranks_out.ptr, sizeof(float) * V, cudaMemcpyDeviceToHost, dev.stream),
                  "copy ranks to host");
-        GCU_TRY(dev.sync());
     }
+    GCU_TRY(dev.sync());
     *iterations = iters;
     *converged = p.host_state->done != 0;
     return ok();
