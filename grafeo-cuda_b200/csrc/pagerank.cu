@@ -368,8 +368,12 @@ __global__ void __launch_bounds__(kPrThreads) pr_rows_kernel(
     }
 }
 
-// Finishes the long rows from their segment partials (in segment order), then
-// the last block reduces all partials in a fixed order and advances the state.
+// Finishes the long rows from their segment partials (in segment order) and
+// folds a fixed slice of kFinSlice row-kernel block partials per block; then
+// the last block reduces the per-block results in a fixed order and advances
+// the state.
+constexpr uint32_t kFinSlice = 2048;
+
 __global__ void __launch_bounds__(256) pr_finish_kernel(
     const uint32_t* __restrict__ poff, uint32_t long_rows, const uint32_t* __restrict__ unit_begin,
     const double* __restrict__ seg_partial, const float* __restrict__ rank_in, float* __restrict__ rank_out,
@@ -387,6 +391,11 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(
         for (uint32_t u = unit_begin[i]; u < unit_begin[i + 1]; ++u) sum += seg_partial[u];
         pr_finish_row(i, sum, poff[i + 1] - poff[i], rank_in, rank_out, contrib_out, base, damp, spread, d, g);
     }
+    const uint64_t slice_end = std::min<uint64_t>(static_cast<uint64_t>(blockIdx.x + 1) * kFinSlice, row_blocks);
+    for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * kFinSlice + threadIdx.x; k < slice_end; k += blockDim.x) {
+        d += row_partials[2 * k];
+        g += row_partials[2 * k + 1];
+    }
     d = block_sum(d, scratch);
     g = block_sum(g, scratch);
     if (threadIdx.x == 0) {
@@ -400,10 +409,6 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(
     if (!s_last) return;
     __threadfence();
     double dd = 0.0, gg = 0.0;
-    for (uint32_t k = threadIdx.x; k < row_blocks; k += blockDim.x) {
-        dd += __ldcg(row_partials + 2 * k);
-        gg += __ldcg(row_partials + 2 * k + 1);
-    }
     for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
         dd += __ldcg(fin_partials + 2 * k);
         gg += __ldcg(fin_partials + 2 * k + 1);
@@ -520,7 +525,8 @@ static Error ensure_plan(GraphImpl& g) {
     }
     add(kPhaseEmpty, begin[0], end[0], 0, 0, static_cast<uint32_t>(ceil_div_u64(p.empty_rows, kPrThreads)));
     s.total_blocks = blocks;
-    p.fin_blocks = static_cast<uint32_t>(std::max<uint64_t>(1, ceil_div_u64(p.long_rows, 256)));
+    p.fin_blocks = static_cast<uint32_t>(
+        std::max<uint64_t>({1, ceil_div_u64(p.long_rows, 256), ceil_div_u64(blocks, kFinSlice)}));
 
     GCU_TRY(p.ranks.allocate(dev, 2 * static_cast<uint64_t>(V)));
     GCU_TRY(p.contrib.allocate(dev, 2 * static_cast<uint64_t>(V)));
