@@ -16,14 +16,13 @@
 //    hit L1/L2 lines that are already hot. The relabelled CSR keeps every
 //    list in its original order, so each row's summation order is the
 //    original one.
-//  * Rows of one class have similar length, so a block takes a run of
-//    consecutive rows of one class holding at most 4096 entries, gathers
-//    their contributions with one flat coalesced loop (4 loads in flight per
-//    thread, no per-row dependency chain) into shared memory, and sums every
-//    row there with about deg/8 threads. No search and no carries. Rows of
-//    4096 or more entries are split into 4096-entry segments, one block each,
-//    and their partial sums are added in segment order by the finishing
-//    kernel.
+//  * Rows of one class have similar length, so each class gets a fixed group
+//    of 2^(c-1) lanes per row (1 to 32); a group works on 4 rows in lockstep
+//    so every lane keeps 8 independent loads in flight, consecutive groups read
+//    consecutive rows (coalesced), and there is no search, staging, barrier or
+//    carry. Rows of 4096 or more entries are split into 4096-entry segments,
+//    one block each, and their partial sums are added in segment order by the
+//    finishing kernel.
 //  * Row sums: FP32 Kahan sums per lane, FP64 across lanes (shuffle tree) and
 //    across segments. Epilogue per row v: r'[v] = (1-d)/N + d (sum +
 //    dangling/N); |r' - r| and the dangling mass of r' go to FP64 per-block
@@ -48,7 +47,7 @@ constexpr int kLongClass = 13;        // degree >= 4096
 constexpr uint32_t kSegment = 4096;   // entries per long-row segment (one block)
 constexpr int kClassBlock = 1024;     // vertices per block of the class partition
 constexpr int kMaxPhases = 16;
-constexpr uint32_t kFlatBudget = 4096;  // entries per block for rows below kLongClass
+constexpr int kRowsPerGroup = 4;      // rows a lane group works on in lockstep
 
 enum : uint32_t { kPhaseLong = 0, kPhaseGroup = 1, kPhaseEmpty = 2 };
 
@@ -56,8 +55,8 @@ struct PrPhase {
     uint32_t first_block;  // first block of this phase
     uint32_t row_begin, row_end;
     uint32_t kind;
-    uint32_t log2g;        // threads per row = 1 << log2g (group phases)
-    uint32_t rows_per_group;  // rows per block (group phases)
+    uint32_t log2g;        // lanes per row = 1 << log2g (group phases)
+    uint32_t rows_per_group;  // rows a lane group works on together (group phases)
 };
 
 struct PrSchedule {
@@ -259,9 +258,6 @@ __global__ void __launch_bounds__(kPrThreads) pr_rows_kernel(
     const uint2* __restrict__ units, double* __restrict__ seg_partial, double* __restrict__ row_partials) {
     if (state->done) return;
     __shared__ double scratch[32];
-    __shared__ uint32_t s_off[kFlatBudget + 1];
-    __shared__ float s_val[kFlatBudget];
-    __shared__ double s_part[kPrThreads / 32];
     const uint32_t b = blockIdx.x;
     uint32_t pi = 0;
     while (pi + 1 < sched.nphases && sched.phase[pi + 1].first_block <= b) ++pi;
@@ -277,75 +273,72 @@ __global__ void __launch_bounds__(kPrThreads) pr_rows_kernel(
         const uint32_t s1 = min(s0 + kSegment, row_end);
         float acc = 0.f, comp = 0.f;
         uint32_t j = s0 + threadIdx.x;
-        for (; j + 3 * kPrThreads < s1; j += 4 * kPrThreads) {
-            const uint32_t t0 = ld_stream(ptgt + j), t1 = ld_stream(ptgt + j + kPrThreads);
-            const uint32_t t2 = ld_stream(ptgt + j + 2 * kPrThreads), t3 = ld_stream(ptgt + j + 3 * kPrThreads);
-            const float c0 = __ldg(contrib_in + t0), c1 = __ldg(contrib_in + t1);
-            const float c2 = __ldg(contrib_in + t2), c3 = __ldg(contrib_in + t3);
-            kahan_add(acc, comp, c0);
-            kahan_add(acc, comp, c1);
-            kahan_add(acc, comp, c2);
-            kahan_add(acc, comp, c3);
+        for (; j + 7 * kPrThreads < s1; j += 8 * kPrThreads) {
+            uint32_t t[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) t[q] = ld_stream(ptgt + j + q * kPrThreads);
+            float c[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) c[q] = __ldg(contrib_in + t[q]);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) kahan_add(acc, comp, c[q]);
         }
         for (; j < s1; j += kPrThreads) kahan_add(acc, comp, __ldg(contrib_in + ld_stream(ptgt + j)));
         const double part = block_sum(static_cast<double>(acc) - static_cast<double>(comp), scratch);
         if (threadIdx.x == 0) seg_partial[b - ph.first_block] = part;
     } else if (ph.kind == kPhaseGroup) {
-        // A run of consecutive rows of one class holding at most kFlatBudget
-        // entries: their contributions are gathered by a flat, coalesced loop
-        // with 4 loads in flight per thread into shared memory, then every
-        // row is summed there by 2^log2t threads (Kahan per thread, FP64
-        // shuffle tree across them).
-        const uint32_t rb = ph.row_begin + (b - ph.first_block) * ph.rows_per_group;
-        const uint32_t nrows = min(rb + ph.rows_per_group, ph.row_end) - rb;
-        for (uint32_t k = threadIdx.x; k <= nrows; k += kPrThreads) s_off[k] = poff[rb + k];
-        __syncthreads();
-        const uint32_t z0 = s_off[0];
-        const uint32_t nnz = s_off[nrows] - z0;
-        for (uint32_t k0 = threadIdx.x; k0 < nnz; k0 += 4 * kPrThreads) {
-            uint32_t t[4];
+        // Rows of one class, 2^log2g lanes per row, kRowsPerGroup rows per
+        // group worked on in lockstep: each step issues one target load and
+        // one gather per row (8 in flight per lane with the 2-step unroll),
+        // so no row waits on the previous one's memory round trips.
+        const uint32_t log2g = ph.log2g, g = 1u << log2g;
+        const uint32_t groups = kPrThreads >> log2g;
+        const uint32_t group = threadIdx.x >> log2g, lig = threadIdx.x & (g - 1);
+        const uint32_t first = ph.row_begin + (b - ph.first_block) * groups * kRowsPerGroup;
+        uint32_t rs[kRowsPerGroup], re[kRowsPerGroup];
+        uint32_t longest = 0;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t k = k0 + q * kPrThreads;
-                t[q] = k < nnz ? ld_stream(ptgt + z0 + k) : 0u;
+        for (int q = 0; q < kRowsPerGroup; ++q) {
+            const uint32_t row = first + q * groups + group;
+            rs[q] = 0;
+            re[q] = 0;
+            if (row < ph.row_end) {
+                rs[q] = poff[row];
+                re[q] = poff[row + 1];
+            }
+            longest = max(longest, re[q] - rs[q]);
+        }
+        float acc[kRowsPerGroup], comp[kRowsPerGroup];
+#pragma unroll
+        for (int q = 0; q < kRowsPerGroup; ++q) {
+            acc[q] = 0.f;
+            comp[q] = 0.f;
+        }
+        for (uint32_t off = lig; off < longest; off += 2 * g) {
+            uint32_t t[2][kRowsPerGroup];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+#pragma unroll
+                for (int q = 0; q < kRowsPerGroup; ++q) {
+                    const uint32_t j = rs[q] + off + u * g;
+                    t[u][q] = j < re[q] ? ld_stream(ptgt + j) : 0xFFFFFFFFu;
+                }
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t k = k0 + q * kPrThreads;
-                if (k < nnz) s_val[k] = __ldg(contrib_in + t[q]);
+            for (int u = 0; u < 2; ++u) {
+#pragma unroll
+                for (int q = 0; q < kRowsPerGroup; ++q) {
+                    if (t[u][q] != 0xFFFFFFFFu) kahan_add(acc[q], comp[q], __ldg(contrib_in + t[u][q]));
+                }
             }
         }
-        __syncthreads();
-        const uint32_t log2t = ph.log2g, T = 1u << log2t;
-        const uint32_t per = kPrThreads >> log2t;  // rows summed per pass
-        const uint32_t slot = threadIdx.x >> log2t, lit = threadIdx.x & (T - 1);
-        for (uint32_t r0 = 0; r0 < nrows; r0 += per) {
-            const uint32_t row = r0 + slot;
-            float acc = 0.f, comp = 0.f;
-            uint32_t deg = 0;
-            if (row < nrows) {
-                const uint32_t a = s_off[row] - z0, e = s_off[row + 1] - z0;
-                deg = e - a;
-                for (uint32_t j = a + lit; j < e; j += T) kahan_add(acc, comp, s_val[j]);
-            }
-            double v = static_cast<double>(acc) - static_cast<double>(comp);
-            if (T <= 32) {
-                v = group_sum(v, log2t);
-                if (lit == 0 && row < nrows)
-                    pr_finish_row(rb + row, v, deg, rank_in, rank_out, contrib_out, base, damp, spread, my_diff,
-                                  my_dangle);
-            } else {
-                v = group_sum(v, 5);
-                if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = v;
-                __syncthreads();
-                if (lit == 0 && row < nrows) {
-                    double sum = 0.0;
-                    for (uint32_t w = 0; w < (T >> 5); ++w) sum += s_part[slot * (T >> 5) + w];
-                    pr_finish_row(rb + row, sum, deg, rank_in, rank_out, contrib_out, base, damp, spread, my_diff,
-                                  my_dangle);
-                }
-                __syncthreads();
-            }
+#pragma unroll
+        for (int q = 0; q < kRowsPerGroup; ++q) {
+            const uint32_t row = first + q * groups + group;
+            const double v = group_sum(static_cast<double>(acc[q]) - static_cast<double>(comp[q]), log2g);
+            if (lig == 0 && row < ph.row_end)
+                pr_finish_row(row, v, re[q] - rs[q], rank_in, rank_out, contrib_out, base, damp, spread, my_diff,
+                              my_dangle);
         }
     } else {
         // Rows without entries: the teleport and dangling share only.
@@ -510,12 +503,11 @@ static Error ensure_plan(GraphImpl& g) {
     };
     add(kPhaseLong, 0, p.long_rows, 0, 0, static_cast<uint32_t>(units.size()));
     for (int c = kLongClass - 1; c >= 1; --c) {
-        // Rows of class c have at most 2^c - 1 entries: a block takes as many
-        // as fit kFlatBudget entries, and sums each with about deg/8 threads.
+        // Class c (degrees [2^(c-1), 2^c)): 2^(c-1) lanes per row up to a warp.
         const uint32_t rows = end[c] - begin[c];
-        const uint32_t per_block = kFlatBudget / ((1u << c) - 1);
-        const uint32_t log2t = static_cast<uint32_t>(std::min(8, std::max(0, c - 3)));
-        add(kPhaseGroup, begin[c], end[c], log2t, per_block, static_cast<uint32_t>(ceil_div_u64(rows, per_block)));
+        const uint32_t log2g = std::min<uint32_t>(static_cast<uint32_t>(c - 1), 5);
+        const uint32_t per_block = (kPrThreads >> log2g) * kRowsPerGroup;
+        add(kPhaseGroup, begin[c], end[c], log2g, kRowsPerGroup, static_cast<uint32_t>(ceil_div_u64(rows, per_block)));
     }
     add(kPhaseEmpty, begin[0], end[0], 0, 0, static_cast<uint32_t>(ceil_div_u64(p.empty_rows, kPrThreads)));
     s.total_blocks = blocks;
