@@ -17,8 +17,9 @@
 //    list in its original order, so each row's summation order is the
 //    original one.
 //  * Rows of one class have similar length, so each class gets a fixed group
-//    of 2^(c-1) lanes per row (1 to 32); a group works on 4 rows in lockstep
-//    so every lane keeps 8 independent loads in flight, consecutive groups read
+//    of 2^(c-1) lanes per row (1 to 32); a group works on 2 rows in lockstep,
+//    4 steps per trip, so every lane keeps 8 independent loads in flight within
+//    32 registers (8 CTAs per SM, persistent); consecutive groups read
 //    consecutive rows (coalesced), and there is no search, staging, barrier or
 //    carry. Rows of 4096 or more entries are split into 4096-entry segments,
 //    one block each, and their partial sums are added in segment order by the
@@ -47,7 +48,9 @@ constexpr int kLongClass = 13;        // degree >= 4096
 constexpr uint32_t kSegment = 4096;   // entries per long-row segment (one block)
 constexpr int kClassBlock = 1024;     // vertices per block of the class partition
 constexpr int kMaxPhases = 16;
-constexpr int kRowsPerGroup = 4;      // rows a lane group works on in lockstep
+constexpr int kRowsPerGroup = 2;      // rows a lane group works on in lockstep
+constexpr int kUnroll = 4;            // steps per loop trip: kRowsPerGroup * kUnroll loads in flight
+constexpr int kRowCtasPerSm = 8;      // persistent CTAs of the row kernel per SM
 
 enum : uint32_t { kPhaseLong = 0, kPhaseGroup = 1, kPhaseEmpty = 2 };
 
@@ -78,6 +81,7 @@ struct PageRankPlan {
     uint32_t long_rows = 0;   // rows [0, long_rows) of the relabelled CSR have >= 4096 entries
     uint32_t empty_rows = 0;  // rows without entries (the last class)
     uint32_t fin_blocks = 1;
+    uint32_t row_ctas = 1;    // persistent CTAs of the row kernel
     PrSchedule sched{};
     DeviceBuffer<uint32_t> perm;       // new id -> original id
     DeviceBuffer<uint32_t> inv;        // original id -> new id
@@ -251,19 +255,22 @@ __device__ __forceinline__ double group_sum(double v, uint32_t log2g) {
     return v;
 }
 
-__global__ void __launch_bounds__(kPrThreads) pr_rows_kernel(
+// Persistent: each CTA walks the schedule's work blocks b = blockIdx.x,
+// blockIdx.x + gridDim.x, ... (a fixed assignment, so the per-CTA partial sums
+// are deterministic). 8 CTAs of 256 threads per SM (32 registers).
+__global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
     const uint32_t* __restrict__ poff, const uint32_t* __restrict__ ptgt, const float* __restrict__ rank_in,
     const float* __restrict__ contrib_in, float* __restrict__ rank_out, float* __restrict__ contrib_out, uint32_t V,
     double base, double damp, const PrState* __restrict__ state, const PrSchedule sched,
     const uint2* __restrict__ units, double* __restrict__ seg_partial, double* __restrict__ row_partials) {
     if (state->done) return;
     __shared__ double scratch[32];
-    const uint32_t b = blockIdx.x;
+    const double spread = state->dangling / static_cast<double>(V);
+    double my_diff = 0.0, my_dangle = 0.0;
+    for (uint32_t b = blockIdx.x; b < sched.total_blocks; b += gridDim.x) {
     uint32_t pi = 0;
     while (pi + 1 < sched.nphases && sched.phase[pi + 1].first_block <= b) ++pi;
     const PrPhase ph = sched.phase[pi];
-    const double spread = state->dangling / static_cast<double>(V);
-    double my_diff = 0.0, my_dangle = 0.0;
 
     if (ph.kind == kPhaseLong) {
         // One segment of a long row: 16 entries per thread, 4 loads in flight.
@@ -289,8 +296,8 @@ __global__ void __launch_bounds__(kPrThreads) pr_rows_kernel(
     } else if (ph.kind == kPhaseGroup) {
         // Rows of one class, 2^log2g lanes per row, kRowsPerGroup rows per
         // group worked on in lockstep: each step issues one target load and
-        // one gather per row (8 in flight per lane with the 2-step unroll),
-        // so no row waits on the previous one's memory round trips.
+        // one gather per row (8 in flight per lane with the kUnroll-step
+        // unroll), so no row waits on the previous one's memory round trips.
         const uint32_t log2g = ph.log2g, g = 1u << log2g;
         const uint32_t groups = kPrThreads >> log2g;
         const uint32_t group = threadIdx.x >> log2g, lig = threadIdx.x & (g - 1);
@@ -314,10 +321,10 @@ __global__ void __launch_bounds__(kPrThreads) pr_rows_kernel(
             acc[q] = 0.f;
             comp[q] = 0.f;
         }
-        for (uint32_t off = lig; off < longest; off += 2 * g) {
-            uint32_t t[2][kRowsPerGroup];
+        for (uint32_t off = lig; off < longest; off += kUnroll * g) {
+            uint32_t t[kUnroll][kRowsPerGroup];
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
+            for (int u = 0; u < kUnroll; ++u) {
 #pragma unroll
                 for (int q = 0; q < kRowsPerGroup; ++q) {
                     const uint32_t j = rs[q] + off + u * g;
@@ -325,7 +332,7 @@ __global__ void __launch_bounds__(kPrThreads) pr_rows_kernel(
                 }
             }
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
+            for (int u = 0; u < kUnroll; ++u) {
 #pragma unroll
                 for (int q = 0; q < kRowsPerGroup; ++q) {
                     if (t[u][q] != 0xFFFFFFFFu) kahan_add(acc[q], comp[q], __ldg(contrib_in + t[u][q]));
@@ -346,11 +353,12 @@ __global__ void __launch_bounds__(kPrThreads) pr_rows_kernel(
         if (row < ph.row_end)
             pr_finish_row(row, 0.0, 0, rank_in, rank_out, contrib_out, base, damp, spread, my_diff, my_dangle);
     }
+    }
     my_diff = block_sum(my_diff, scratch);
     my_dangle = block_sum(my_dangle, scratch);
     if (threadIdx.x == 0) {
-        row_partials[2 * b] = my_diff;
-        row_partials[2 * b + 1] = my_dangle;
+        row_partials[2 * blockIdx.x] = my_diff;
+        row_partials[2 * blockIdx.x + 1] = my_dangle;
     }
 }
 
@@ -511,13 +519,14 @@ static Error ensure_plan(GraphImpl& g) {
     }
     add(kPhaseEmpty, begin[0], end[0], 0, 0, static_cast<uint32_t>(ceil_div_u64(p.empty_rows, kPrThreads)));
     s.total_blocks = blocks;
+    p.row_ctas = std::max<uint32_t>(1, std::min<uint32_t>(blocks, static_cast<uint32_t>(dev.sm_count) * kRowCtasPerSm));
     p.fin_blocks = static_cast<uint32_t>(
-        std::max<uint64_t>({1, ceil_div_u64(p.long_rows, 256), ceil_div_u64(blocks, kFinSlice)}));
+        std::max<uint64_t>({1, ceil_div_u64(p.long_rows, 256), ceil_div_u64(p.row_ctas, kFinSlice)}));
 
     GCU_TRY(p.ranks.allocate(dev, 2 * static_cast<uint64_t>(V)));
     GCU_TRY(p.contrib.allocate(dev, 2 * static_cast<uint64_t>(V)));
     GCU_TRY(p.ranks_out.allocate(dev, V));
-    GCU_TRY(p.row_partials.allocate(dev, 2 * static_cast<uint64_t>(std::max<uint32_t>(blocks, 1))));
+    GCU_TRY(p.row_partials.allocate(dev, 2 * static_cast<uint64_t>(p.row_ctas)));
     GCU_TRY(p.fin_partials.allocate(dev, 2 * static_cast<uint64_t>(p.fin_blocks)));
     GCU_TRY(p.state.allocate(dev, 1));
     GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p.host_state), sizeof(PrState)), "cudaMallocHost");
@@ -569,12 +578,12 @@ Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float toler
             const uint32_t it = launched + i;
             const int in = it & 1, out = in ^ 1;
             err = [&]() -> Error {
-                GCU_LAUNCH(dev, "pr_rows", pr_rows_kernel, p.sched.total_blocks, kPrThreads, 0, p.poff.ptr,
+                GCU_LAUNCH(dev, "pr_rows", pr_rows_kernel, p.row_ctas, kPrThreads, 0, p.poff.ptr,
                            p.ptgt.ptr, ranks[in], contrib[in], ranks[out], contrib[out], V, base, damp, p.state.ptr,
                            p.sched, p.units.ptr, p.seg_partial.ptr, p.row_partials.ptr);
                 GCU_LAUNCH(dev, "pr_finish", pr_finish_kernel, p.fin_blocks, 256, 0, p.poff.ptr, p.long_rows,
                            p.unit_begin.ptr, p.seg_partial.ptr, ranks[in], ranks[out], contrib[out], V, base, damp,
-                           p.state.ptr, tol, p.row_partials.ptr, p.sched.total_blocks, p.fin_partials.ptr);
+                           p.state.ptr, tol, p.row_partials.ptr, p.row_ctas, p.fin_partials.ptr);
                 return ok();
             }();
         }

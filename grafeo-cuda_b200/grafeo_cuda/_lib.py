@@ -9,7 +9,9 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libgrafeo_cuda.so")
+# GRAFEO_CUDA_LIBRARY may name another build of the same C ABI (for example a
+# build with different compile-time tuning); the default is the in-place build.
+LIB_PATH = os.environ.get("GRAFEO_CUDA_LIBRARY") or os.path.join(_HERE, "libgrafeo_cuda.so")
 
 u32p = C.POINTER(C.c_uint32)
 i32p = C.POINTER(C.c_int32)
