@@ -60,6 +60,10 @@ SIGNATURES = {
     "gcu_graph_destroy": (None, [C.c_void_p]),
     "gcu_triangle_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "gcu_triangle_count_oriented": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
+    "gcu_triangle_count_oriented_noalloc": (
+        C.c_int,
+        [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.POINTER(C.c_uint64)],
+    ),
     "gcu_bfs": (
         C.c_int,
         [C.c_void_p, C.c_uint32, i32p, C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.POINTER(C.c_double)],

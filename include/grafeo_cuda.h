@@ -146,6 +146,24 @@ GCU_API gcu_status gcu_triangle_count(gcu_graph* g, uint64_t* total, double* sec
 GCU_API gcu_status gcu_triangle_count_oriented(gcu_graph* g, uint64_t* total,
                                                double* seconds);
 
+/* Allocation-free oriented triangle count. No counterpart in the reference.
+ * For callers that cannot allocate device memory when they need the count
+ * (a process whose memory pool owns the whole device, a framework allocator
+ * that forbids side allocations, a path where an allocation may block or fail
+ * late): the same count as gcu_triangle_count_oriented over a CSR the caller
+ * already holds on the device (d_offsets: num_nodes + 1 u32, d_targets:
+ * num_edges u32, valid per validate_csr; not checked here), run on `stream`
+ * (NULL: the default stream) of the calling thread's current device, result
+ * in *total (host). Its only working memory is a fixed 4 MiB array inside the
+ * library, present on every device that loads it until exit; it calls no
+ * cudaMalloc/cudaFree. At most 1,048,576 nodes (else GCU_ERR_KERNEL). All
+ * calls on a device share that array: calls that overlap on the GPU race.
+ * The first call on a device looks the array up (cudaGetSymbolAddress); make
+ * it before any stream capture. */
+GCU_API gcu_status gcu_triangle_count_oriented_noalloc(const uint32_t* d_offsets, const uint32_t* d_targets,
+                                                       uint32_t num_nodes, uint32_t num_edges, void* stream,
+                                                       uint64_t* total);
+
 /* bfs::bfs(graph, source) (bfs.rs:42-131). distances (num_nodes i32, -1 =
  * unreachable) may be NULL, in which case the distances stay on the device.
  * A source >= num_nodes is GCU_ERR_KERNEL. */
