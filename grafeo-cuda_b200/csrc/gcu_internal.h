@@ -165,6 +165,7 @@ struct GraphImpl {
     std::mutex mu;  // guards the lazily built caches below
     int symmetric = -1;  // every entry u -> v has v -> u: -1 unknown, 0 no, 1 yes
     PageRankPlan* pr_plan = nullptr;  // owned; freed by destroy_pagerank_plan
+    PageRankPlan* pr_plan_directed = nullptr;  // pull over the transpose; owned
     BfsWork* bfs_work = nullptr;      // owned; freed by destroy_bfs_work
     ~GraphImpl();
 };
@@ -210,6 +211,22 @@ Error k_truss(GraphImpl& g, uint32_t k, std::vector<uint32_t>* edges, uint32_t* 
 // Exclusive scan of u32 counts into u32 offsets (out has n + 1 entries);
 // returns the total through the device (out[n]).
 Error exclusive_scan_u32(DeviceImpl& dev, const uint32_t* d_in, uint32_t* d_out, uint64_t n);
+
+// Stable LSD radix sort of n 64-bit keys by bits [low_bit, high_bit), 8 per
+// pass, ping-ponging between keys and tmp; *sorted is whichever holds the result.
+Error radix_sort_u64(DeviceImpl& dev, uint64_t* keys, uint64_t* tmp, uint64_t n, uint32_t low_bit, uint32_t high_bit,
+                     uint64_t** sorted);
+
+// In-lists of a CSR (the transpose), every in-list ordered by source.
+Error transpose_csr(DeviceImpl& dev, const uint32_t* offsets, const uint32_t* targets, uint32_t V, uint32_t E,
+                    DeviceBuffer<uint32_t>* t_offsets, DeviceBuffer<uint32_t>* t_targets);
+
+// PageRank over the CSR lists (directed = false: symmetric graph, pagerank.rs)
+// or over their transpose with out-degrees from the lists (directed = true).
+// tele (nullable, V floats, original ids): personalisation vector that takes
+// the teleport and the dangling mass instead of the uniform 1/N.
+Error pagerank_ex(GraphImpl& g, bool directed, const float* tele, float damping, uint32_t max_iterations,
+                  float tolerance, float* host_ranks, uint32_t* iterations, bool* converged);
 
 void destroy_pagerank_plan(PageRankPlan* p);
 void destroy_bfs_work(BfsWork* w);

@@ -80,6 +80,7 @@ struct PrState {
 struct PageRankPlan {
     uint32_t long_rows = 0;   // rows [0, long_rows) of the relabelled CSR have >= 4096 entries
     uint32_t empty_rows = 0;  // rows without entries (the last class)
+    uint32_t dangling_rows = 0;  // vertices without out-edges
     uint32_t fin_blocks = 1;
     uint32_t row_ctas = 1;    // persistent CTAs of the row kernel
     PrSchedule sched{};
@@ -87,6 +88,7 @@ struct PageRankPlan {
     DeviceBuffer<uint32_t> inv;        // original id -> new id
     DeviceBuffer<uint32_t> poff;       // relabelled offsets (V + 1)
     DeviceBuffer<uint32_t> ptgt;       // relabelled targets (E)
+    DeviceBuffer<uint32_t> outdeg;     // out-degrees, relabelled order (only when pulling over the transpose)
     DeviceBuffer<uint2> units;         // long-row segments: (row, segment)
     DeviceBuffer<uint32_t> unit_begin; // long row i owns units [unit_begin[i], unit_begin[i+1])
     DeviceBuffer<double> seg_partial;  // one partial sum per unit
@@ -209,13 +211,38 @@ __global__ void __launch_bounds__(256) pr_perm_fill_kernel(const uint32_t* __res
     }
 }
 
-__global__ void pr_init_kernel(const uint32_t* __restrict__ poff, uint32_t V, float r0, float* __restrict__ ranks,
-                               float* __restrict__ contrib) {
+__global__ void pr_init_kernel(const uint32_t* __restrict__ poff, const uint32_t* __restrict__ outdeg, uint32_t V,
+                               float r0, float* __restrict__ ranks, float* __restrict__ contrib) {
     for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
          v += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint32_t deg = poff[v + 1] - poff[v];
+        const uint32_t deg = outdeg ? outdeg[v] : poff[v + 1] - poff[v];
         ranks[v] = r0;
         contrib[v] = deg > 0 ? r0 / static_cast<float>(deg) : 0.f;
+    }
+}
+
+// Out-degrees from the original CSR, in relabelled order; counts the vertices
+// without out-edges (the dangling ones).
+__global__ void pr_outdeg_kernel(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ perm, uint32_t V,
+                                 uint32_t* __restrict__ outdeg, uint32_t* __restrict__ dangling_count) {
+    uint32_t zeros = 0;
+    for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < V;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t u = perm[r];
+        const uint32_t d = offsets[u + 1] - offsets[u];
+        outdeg[r] = d;
+        zeros += d == 0 ? 1u : 0u;
+    }
+    zeros = warp_sum(zeros);
+    if (lane_id() == 0 && zeros) atomicAdd(dangling_count, zeros);
+}
+
+// Personalisation vector in relabelled order.
+__global__ void pr_permute_tele_kernel(const float* __restrict__ tele, const uint32_t* __restrict__ perm, uint32_t V,
+                                       float* __restrict__ out) {
+    for (uint64_t r = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; r < V;
+         r += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        out[r] = tele[perm[r]];
     }
 }
 
@@ -229,12 +256,24 @@ __global__ void pr_unpermute_kernel(const float* __restrict__ ranks, const uint3
 
 // ---------------------------------------------------------------- iteration kernels
 
-// Row update shared by the row and finishing kernels.
-__device__ __forceinline__ void pr_finish_row(uint32_t v, double sum, uint32_t deg, const float* __restrict__ rank_in,
-                                              float* __restrict__ rank_out, float* __restrict__ contrib_out,
-                                              double base, double damp, double spread, double& diff,
-                                              double& dangle) {
-    const float r = static_cast<float>(base + damp * (sum + spread));
+// Row update shared by the row and finishing kernels. row_len is the length
+// of the pulled row; the out-degree is that length (symmetric graph) or
+// outdeg[v] (pull over the transpose). Uniform teleport: r = (1-d)/N +
+// d (sum + dangling/N); with a personalisation vector p: r = (1-d) p[v] +
+// d (sum + dangling p[v]).
+__device__ __forceinline__ void pr_finish_row(uint32_t v, double sum, uint32_t row_len,
+                                              const float* __restrict__ rank_in, float* __restrict__ rank_out,
+                                              float* __restrict__ contrib_out, const uint32_t* __restrict__ outdeg,
+                                              const float* __restrict__ tele, double base, double damp,
+                                              double spread, double dangling, double& diff, double& dangle) {
+    const uint32_t deg = outdeg ? outdeg[v] : row_len;
+    float r;
+    if (tele) {
+        const double pv = static_cast<double>(tele[v]);
+        r = static_cast<float>((1.0 - damp) * pv + damp * (sum + dangling * pv));
+    } else {
+        r = static_cast<float>(base + damp * (sum + spread));
+    }
     const float old = rank_in[v];
     diff += fabs(static_cast<double>(r) - static_cast<double>(old));
     rank_out[v] = r;
@@ -260,12 +299,14 @@ __device__ __forceinline__ double group_sum(double v, uint32_t log2g) {
 // are deterministic). 8 CTAs of 256 threads per SM (32 registers).
 __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
     const uint32_t* __restrict__ poff, const uint32_t* __restrict__ ptgt, const float* __restrict__ rank_in,
-    const float* __restrict__ contrib_in, float* __restrict__ rank_out, float* __restrict__ contrib_out, uint32_t V,
-    double base, double damp, const PrState* __restrict__ state, const PrSchedule sched,
+    const float* __restrict__ contrib_in, float* __restrict__ rank_out, float* __restrict__ contrib_out,
+    const uint32_t* __restrict__ outdeg, const float* __restrict__ tele, uint32_t V, double base, double damp,
+    const PrState* __restrict__ state, const PrSchedule sched,
     const uint2* __restrict__ units, double* __restrict__ seg_partial, double* __restrict__ row_partials) {
     if (state->done) return;
     __shared__ double scratch[32];
-    const double spread = state->dangling / static_cast<double>(V);
+    const double dangling = state->dangling;
+    const double spread = dangling / static_cast<double>(V);
     double my_diff = 0.0, my_dangle = 0.0;
     for (uint32_t b = blockIdx.x; b < sched.total_blocks; b += gridDim.x) {
     uint32_t pi = 0;
@@ -344,14 +385,14 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
             const uint32_t row = first + q * groups + group;
             const double v = group_sum(static_cast<double>(acc[q]) - static_cast<double>(comp[q]), log2g);
             if (lig == 0 && row < ph.row_end)
-                pr_finish_row(row, v, re[q] - rs[q], rank_in, rank_out, contrib_out, base, damp, spread, my_diff,
+                pr_finish_row(row, v, re[q] - rs[q], rank_in, rank_out, contrib_out, outdeg, tele, base, damp, spread, dangling, my_diff,
                               my_dangle);
         }
     } else {
         // Rows without entries: the teleport and dangling share only.
         const uint32_t row = ph.row_begin + (b - ph.first_block) * kPrThreads + threadIdx.x;
         if (row < ph.row_end)
-            pr_finish_row(row, 0.0, 0, rank_in, rank_out, contrib_out, base, damp, spread, my_diff, my_dangle);
+            pr_finish_row(row, 0.0, 0, rank_in, rank_out, contrib_out, outdeg, tele, base, damp, spread, dangling, my_diff, my_dangle);
     }
     }
     my_diff = block_sum(my_diff, scratch);
@@ -371,19 +412,21 @@ constexpr uint32_t kFinSlice = 2048;
 __global__ void __launch_bounds__(256) pr_finish_kernel(
     const uint32_t* __restrict__ poff, uint32_t long_rows, const uint32_t* __restrict__ unit_begin,
     const double* __restrict__ seg_partial, const float* __restrict__ rank_in, float* __restrict__ rank_out,
-    float* __restrict__ contrib_out, uint32_t V, double base, double damp, PrState* __restrict__ state,
+    float* __restrict__ contrib_out, const uint32_t* __restrict__ outdeg, const float* __restrict__ tele, uint32_t V,
+    double base, double damp, PrState* __restrict__ state,
     double tolerance, const double* __restrict__ row_partials, uint32_t row_blocks,
     double* __restrict__ fin_partials) {
     if (state->done) return;
     __shared__ double scratch[32];
     __shared__ bool s_last;
-    const double spread = state->dangling / static_cast<double>(V);
+    const double dangling = state->dangling;
+    const double spread = dangling / static_cast<double>(V);
     double d = 0.0, g = 0.0;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < long_rows) {
         double sum = 0.0;
         for (uint32_t u = unit_begin[i]; u < unit_begin[i + 1]; ++u) sum += seg_partial[u];
-        pr_finish_row(i, sum, poff[i + 1] - poff[i], rank_in, rank_out, contrib_out, base, damp, spread, d, g);
+        pr_finish_row(i, sum, poff[i + 1] - poff[i], rank_in, rank_out, contrib_out, outdeg, tele, base, damp, spread, dangling, d, g);
     }
     const uint64_t slice_end = std::min<uint64_t>(static_cast<uint64_t>(blockIdx.x + 1) * kFinSlice, row_blocks);
     for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * kFinSlice + threadIdx.x; k < slice_end; k += blockDim.x) {
@@ -420,8 +463,12 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(
 
 // ---------------------------------------------------------------- host
 
-static Error ensure_plan(GraphImpl& g) {
-    if (g.pr_plan) return ok();
+// Builds the relabelled pull CSR and the schedule for pulling over
+// (pull_offsets, pull_targets); `out_offsets`, when given, is the CSR whose
+// list lengths are the out-degrees (the graph itself when pulling over its
+// transpose).
+static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32_t* pull_targets,
+                        const uint32_t* out_offsets, PageRankPlan** out) {
     DeviceImpl& dev = *g.dev;
     auto plan = std::unique_ptr<PageRankPlan, void (*)(PageRankPlan*)>(new PageRankPlan, destroy_pagerank_plan);
     PageRankPlan& p = *plan;
@@ -435,26 +482,32 @@ static Error ensure_plan(GraphImpl& g) {
     DeviceBuffer<uint32_t> counts, cpos, starts;
     GCU_TRY(counts.allocate(dev, ncount));
     GCU_TRY(cpos.allocate(dev, ncount + 1));
-    GCU_TRY(starts.allocate(dev, kDegClasses + 1));
+    GCU_TRY(starts.allocate(dev, kDegClasses + 2));
     GCU_TRY(p.perm.allocate(dev, V));
     GCU_TRY(p.inv.allocate(dev, V));
-    GCU_LAUNCH(dev, "pr_class_count", pr_class_count_kernel, nblk, kClassBlock, 0, g.offsets.ptr, V, nblk,
+    GCU_LAUNCH(dev, "pr_class_count", pr_class_count_kernel, nblk, kClassBlock, 0, pull_offsets, V, nblk,
                counts.ptr);
     GCU_TRY(exclusive_scan_u32(dev, counts.ptr, cpos.ptr, ncount));
-    GCU_LAUNCH(dev, "pr_class_scatter", pr_class_scatter_kernel, nblk, kClassBlock, 0, g.offsets.ptr, V, nblk,
+    GCU_LAUNCH(dev, "pr_class_scatter", pr_class_scatter_kernel, nblk, kClassBlock, 0, pull_offsets, V, nblk,
                cpos.ptr, p.perm.ptr, p.inv.ptr);
+    GCU_CUDA(cudaMemsetAsync(starts.ptr + kDegClasses + 1, 0, sizeof(uint32_t), dev.stream), "memset");
     GCU_LAUNCH(dev, "pr_class_starts", pr_class_starts_kernel, 1, 64, 0, cpos.ptr, nblk, starts.ptr);
 
-    // 2. Relabelled CSR.
+    // 2. Relabelled CSR (and out-degrees when they differ from the row lengths).
     GCU_TRY(p.poff.allocate(dev, static_cast<uint64_t>(V) + 1));
     GCU_TRY(p.ptgt.allocate(dev, E));
-    GCU_LAUNCH(dev, "pr_perm_degree", pr_perm_degree_kernel, vgrid, 256, 0, g.offsets.ptr, p.perm.ptr, V, p.poff.ptr);
+    GCU_LAUNCH(dev, "pr_perm_degree", pr_perm_degree_kernel, vgrid, 256, 0, pull_offsets, p.perm.ptr, V, p.poff.ptr);
     GCU_TRY(exclusive_scan_u32(dev, p.poff.ptr, p.poff.ptr, V));
     if (E > 0) {
-        GCU_LAUNCH(dev, "pr_perm_fill", pr_perm_fill_kernel, vgrid, 256, 0, g.offsets.ptr, g.targets.ptr, p.perm.ptr,
+        GCU_LAUNCH(dev, "pr_perm_fill", pr_perm_fill_kernel, vgrid, 256, 0, pull_offsets, pull_targets, p.perm.ptr,
                    p.inv.ptr, p.poff.ptr, V, p.ptgt.ptr);
     }
-    uint32_t cls[kDegClasses + 1];
+    if (out_offsets) {
+        GCU_TRY(p.outdeg.allocate(dev, V));
+        GCU_LAUNCH(dev, "pr_outdeg", pr_outdeg_kernel, vgrid, 256, 0, out_offsets, p.perm.ptr, V, p.outdeg.ptr,
+                   starts.ptr + kDegClasses + 1);
+    }
+    uint32_t cls[kDegClasses + 2];
     GCU_CUDA(cudaMemcpyAsync(cls, starts.ptr, sizeof(cls), cudaMemcpyDeviceToHost, dev.stream), "copy");
     GCU_TRY(dev.sync());
     // Rows of class c (new ids) are [begin[c], end[c]); classes are laid out
@@ -466,6 +519,7 @@ static Error ensure_plan(GraphImpl& g) {
     }
     p.long_rows = begin[kLongClass - 1];  // classes >= kLongClass occupy [0, begin[kLongClass - 1])
     p.empty_rows = end[0] - begin[0];
+    p.dangling_rows = out_offsets ? cls[kDegClasses + 1] : p.empty_rows;
 
     // 3. Long-row segments.
     std::vector<uint32_t> long_off(p.long_rows + 1, 0);
@@ -531,12 +585,29 @@ static Error ensure_plan(GraphImpl& g) {
     GCU_TRY(p.state.allocate(dev, 1));
     GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p.host_state), sizeof(PrState)), "cudaMallocHost");
     GCU_TRY(dev.sync());
-    g.pr_plan = plan.release();
+    *out = plan.release();
     return ok();
 }
 
-Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float tolerance, float* host_ranks,
-               uint32_t* iterations, bool* converged) {
+static Error ensure_plan(GraphImpl& g, bool directed, PageRankPlan** plan) {
+    PageRankPlan*& slot = directed ? g.pr_plan_directed : g.pr_plan;
+    if (!slot) {
+        if (directed) {
+            // Pull over the in-lists (transpose); out-degrees from the lists.
+            DeviceBuffer<uint32_t> t_offsets, t_targets;
+            GCU_TRY(transpose_csr(*g.dev, g.offsets.ptr, g.targets.ptr, g.num_nodes, g.num_edges, &t_offsets,
+                                  &t_targets));
+            GCU_TRY(build_plan(g, t_offsets.ptr, t_targets.ptr, g.offsets.ptr, &slot));
+        } else {
+            GCU_TRY(build_plan(g, g.offsets.ptr, g.targets.ptr, nullptr, &slot));
+        }
+    }
+    *plan = slot;
+    return ok();
+}
+
+Error pagerank_ex(GraphImpl& g, bool directed, const float* tele_host, float damping, uint32_t max_iterations,
+                  float tolerance, float* host_ranks, uint32_t* iterations, bool* converged) {
     const uint32_t V = g.num_nodes;
     // pagerank.rs:56-63: no nodes, no ranks.
     if (V == 0) {
@@ -545,17 +616,30 @@ Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float toler
         return ok();
     }
     DeviceImpl& dev = *g.dev;
-    GCU_TRY(ensure_plan(g));
-    PageRankPlan& p = *g.pr_plan;
+    PageRankPlan* plan = nullptr;
+    GCU_TRY(ensure_plan(g, directed, &plan));
+    PageRankPlan& p = *plan;
     float* ranks[2] = {p.ranks.ptr, p.ranks.ptr + V};
     float* contrib[2] = {p.contrib.ptr, p.contrib.ptr + V};
     const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
     const unsigned vgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
+    const uint32_t* outdeg = directed ? p.outdeg.ptr : nullptr;
+
+    DeviceBuffer<float> tele_raw, tele;
+    if (tele_host) {
+        GCU_TRY(tele_raw.allocate(dev, V));
+        GCU_TRY(tele.allocate(dev, V));
+        GCU_CUDA(cudaMemcpyAsync(tele_raw.ptr, tele_host, sizeof(float) * V, cudaMemcpyHostToDevice, dev.stream),
+                 "copy personalisation vector");
+        GCU_LAUNCH(dev, "pr_permute_tele", pr_permute_tele_kernel, vgrid, 256, 0, tele_raw.ptr, p.perm.ptr, V,
+                   tele.ptr);
+    }
+    const float* d_tele = tele_host ? tele.ptr : nullptr;
 
     const float r0 = 1.0f / static_cast<float>(V);  // pagerank.rs:83
-    GCU_LAUNCH(dev, "pr_init", pr_init_kernel, vgrid, 256, 0, p.poff.ptr, V, r0, ranks[0], contrib[0]);
+    GCU_LAUNCH(dev, "pr_init", pr_init_kernel, vgrid, 256, 0, p.poff.ptr, outdeg, V, r0, ranks[0], contrib[0]);
     PrState init{};
-    init.dangling = static_cast<double>(p.empty_rows) * static_cast<double>(r0);
+    init.dangling = static_cast<double>(p.dangling_rows) * static_cast<double>(r0);
     init.last_diff = INFINITY;
     *p.host_state = init;
     GCU_CUDA(cudaMemcpyAsync(p.state.ptr, p.host_state, sizeof(PrState), cudaMemcpyHostToDevice, dev.stream), "copy");
@@ -578,12 +662,12 @@ Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float toler
             const uint32_t it = launched + i;
             const int in = it & 1, out = in ^ 1;
             err = [&]() -> Error {
-                GCU_LAUNCH(dev, "pr_rows", pr_rows_kernel, p.row_ctas, kPrThreads, 0, p.poff.ptr,
-                           p.ptgt.ptr, ranks[in], contrib[in], ranks[out], contrib[out], V, base, damp, p.state.ptr,
-                           p.sched, p.units.ptr, p.seg_partial.ptr, p.row_partials.ptr);
+                GCU_LAUNCH(dev, "pr_rows", pr_rows_kernel, p.row_ctas, kPrThreads, 0, p.poff.ptr, p.ptgt.ptr,
+                           ranks[in], contrib[in], ranks[out], contrib[out], outdeg, d_tele, V, base, damp,
+                           p.state.ptr, p.sched, p.units.ptr, p.seg_partial.ptr, p.row_partials.ptr);
                 GCU_LAUNCH(dev, "pr_finish", pr_finish_kernel, p.fin_blocks, 256, 0, p.poff.ptr, p.long_rows,
-                           p.unit_begin.ptr, p.seg_partial.ptr, ranks[in], ranks[out], contrib[out], V, base, damp,
-                           p.state.ptr, tol, p.row_partials.ptr, p.row_ctas, p.fin_partials.ptr);
+                           p.unit_begin.ptr, p.seg_partial.ptr, ranks[in], ranks[out], contrib[out], outdeg, d_tele,
+                           V, base, damp, p.state.ptr, tol, p.row_partials.ptr, p.row_ctas, p.fin_partials.ptr);
                 return ok();
             }();
         }
@@ -614,6 +698,11 @@ Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float toler
     *iterations = iters;
     *converged = p.host_state->done != 0;
     return ok();
+}
+
+Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float tolerance, float* host_ranks,
+               uint32_t* iterations, bool* converged) {
+    return pagerank_ex(g, false, nullptr, damping, max_iterations, tolerance, host_ranks, iterations, converged);
 }
 
 }  // namespace gcu

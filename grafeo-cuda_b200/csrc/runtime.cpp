@@ -152,8 +152,10 @@ GraphImpl::~GraphImpl() {
     if (dev) {
         dev->activate();
         destroy_pagerank_plan(pr_plan);
+        destroy_pagerank_plan(pr_plan_directed);
         destroy_bfs_work(bfs_work);
         pr_plan = nullptr;
+        pr_plan_directed = nullptr;
         bfs_work = nullptr;
         offsets.reset();
         targets.reset();
@@ -448,6 +450,51 @@ GCU_API gcu_status gcu_pagerank(gcu_graph* g, float damping, uint32_t max_iterat
     uint32_t it = 0;
     bool conv = false;
     if (e.ok()) e = pagerank(gi, damping, max_iterations, tolerance, ranks, &it, &conv);
+    if (!e.ok()) return fail(e);
+    if (iterations) *iterations = it;
+    if (converged) *converged = conv ? 1 : 0;
+    if (seconds) *seconds = wall.seconds();
+    return succeed();
+}
+
+GCU_API gcu_status gcu_pagerank_directed(gcu_graph* g, float damping, uint32_t max_iterations, float tolerance,
+                                         float* ranks, uint32_t* iterations, int* converged, double* seconds) {
+    WallTimer wall;
+    if (!g) return fail(kernel_error("graph is NULL"));
+    GraphImpl& gi = *g->impl;
+    std::lock_guard<std::mutex> lock(gi.mu);
+    Error e = gi.dev->activate();
+    uint32_t it = 0;
+    bool conv = false;
+    if (e.ok()) e = pagerank_ex(gi, true, nullptr, damping, max_iterations, tolerance, ranks, &it, &conv);
+    if (!e.ok()) return fail(e);
+    if (iterations) *iterations = it;
+    if (converged) *converged = conv ? 1 : 0;
+    if (seconds) *seconds = wall.seconds();
+    return succeed();
+}
+
+GCU_API gcu_status gcu_personalized_pagerank(gcu_graph* g, const uint32_t* seeds, size_t n_seeds, int directed,
+                                             float damping, uint32_t max_iterations, float tolerance, float* ranks,
+                                             uint32_t* iterations, int* converged, double* seconds) {
+    WallTimer wall;
+    if (!g) return fail(kernel_error("graph is NULL"));
+    GraphImpl& gi = *g->impl;
+    if (n_seeds == 0 || !seeds) return fail(kernel_error("personalized PageRank needs at least one seed"));
+    std::vector<float> tele(gi.num_nodes, 0.f);
+    for (size_t i = 0; i < n_seeds; ++i) {
+        if (seeds[i] >= gi.num_nodes) {
+            return fail(kernel_error("seed node " + std::to_string(seeds[i]) + " out of range (num_nodes = " +
+                                     std::to_string(gi.num_nodes) + ")"));
+        }
+        tele[seeds[i]] += static_cast<float>(1.0 / static_cast<double>(n_seeds));
+    }
+    std::lock_guard<std::mutex> lock(gi.mu);
+    Error e = gi.dev->activate();
+    uint32_t it = 0;
+    bool conv = false;
+    if (e.ok())
+        e = pagerank_ex(gi, directed != 0, tele.data(), damping, max_iterations, tolerance, ranks, &it, &conv);
     if (!e.ok()) return fail(e);
     if (iterations) *iterations = it;
     if (converged) *converged = conv ? 1 : 0;

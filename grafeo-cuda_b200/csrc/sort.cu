@@ -1,0 +1,158 @@
+// Stable LSD radix sort of 64-bit keys, and the CSR transpose built on it.
+//
+// Each pass sorts by one 8-bit digit: per-tile digit histograms (digit-major,
+// so one exclusive scan gives every (digit, tile) its output base), then a
+// stable scatter: a tile of kSortTile keys is walked in rounds of 256 keys in
+// index order, and inside a round every key's rank among the equal digits
+// before it comes from warp matches plus a prefix over the block's warps.
+// Stability makes the sort of (target << 32 | source) keys by their high word
+// keep every in-list ordered by source, so the transpose is deterministic.
+#include <algorithm>
+
+#include "device_common.cuh"
+#include "gcu_internal.h"
+
+namespace gcu {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortRounds = 16;
+constexpr int kSortTile = kSortThreads * kSortRounds;  // keys per tile
+constexpr int kRadix = 256;
+
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t* __restrict__ keys, uint64_t n,
+                                                                  uint32_t shift, uint32_t ntiles,
+                                                                  uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[kRadix];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+    for (int r = 0; r < kSortRounds; ++r) {
+        const uint64_t i = base + static_cast<uint64_t>(r) * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xFF], 1u);
+    }
+    __syncthreads();
+    hist[static_cast<uint64_t>(threadIdx.x) * ntiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint64_t* __restrict__ in,
+                                                                     uint64_t* __restrict__ out, uint64_t n,
+                                                                     uint32_t shift, uint32_t ntiles,
+                                                                     const uint32_t* __restrict__ bases) {
+    __shared__ uint32_t s_base[kRadix];
+    __shared__ uint32_t s_run[kRadix];
+    __shared__ uint32_t s_wcount[kSortThreads / 32][kRadix];
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    s_base[threadIdx.x] = bases[static_cast<uint64_t>(threadIdx.x) * ntiles + blockIdx.x];
+    s_run[threadIdx.x] = 0;
+    for (int w = 0; w < kSortThreads / 32; ++w) s_wcount[w][threadIdx.x] = 0;
+    __syncthreads();
+    const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+    for (int r = 0; r < kSortRounds; ++r) {
+        const uint64_t i = base + static_cast<uint64_t>(r) * kSortThreads + threadIdx.x;
+        const bool valid = i < n;
+        const uint64_t key = valid ? in[i] : 0;
+        const uint32_t d = valid ? static_cast<uint32_t>((key >> shift) & 0xFF) : kRadix;  // kRadix: no key
+        const unsigned same = __match_any_sync(kFullMask, d);
+        const uint32_t rank = __popc(same & ((1u << lane) - 1));
+        if (valid && lane == static_cast<unsigned>(__ffs(same) - 1)) s_wcount[warp][d] = __popc(same);
+        __syncthreads();
+        if (valid) {
+            uint32_t before = 0;
+            for (unsigned w = 0; w < warp; ++w) before += s_wcount[w][d];
+            out[s_base[d] + s_run[d] + before + rank] = key;
+        }
+        __syncthreads();
+        uint32_t round_total = 0;
+        for (int w = 0; w < kSortThreads / 32; ++w) {
+            round_total += s_wcount[w][threadIdx.x];
+            s_wcount[w][threadIdx.x] = 0;
+        }
+        s_run[threadIdx.x] += round_total;
+        __syncthreads();
+    }
+}
+
+Error radix_sort_u64(DeviceImpl& dev, uint64_t* keys, uint64_t* tmp, uint64_t n, uint32_t low_bit, uint32_t high_bit,
+                     uint64_t** sorted) {
+    *sorted = keys;
+    if (n <= 1 || high_bit <= low_bit) return ok();
+    const uint64_t ntiles64 = ceil_div_u64(n, kSortTile);
+    if (ntiles64 * kRadix > 0xFFFFFFFFull || n > 0xFFFFFFFFull) return kernel_error("radix sort input too large");
+    const uint32_t ntiles = static_cast<uint32_t>(ntiles64);
+    DeviceBuffer<uint32_t> hist, bases;
+    GCU_TRY(hist.allocate(dev, static_cast<uint64_t>(ntiles) * kRadix));
+    GCU_TRY(bases.allocate(dev, static_cast<uint64_t>(ntiles) * kRadix + 1));
+    uint64_t* src = keys;
+    uint64_t* dst = tmp;
+    for (uint32_t shift = low_bit; shift < high_bit; shift += 8) {
+        GCU_LAUNCH(dev, "radix_hist", radix_hist_kernel, ntiles, kSortThreads, 0, src, n, shift, ntiles, hist.ptr);
+        GCU_TRY(exclusive_scan_u32(dev, hist.ptr, bases.ptr, static_cast<uint64_t>(ntiles) * kRadix));
+        GCU_LAUNCH(dev, "radix_scatter", radix_scatter_kernel, ntiles, kSortThreads, 0, src, dst, n, shift, ntiles,
+                   bases.ptr);
+        std::swap(src, dst);
+    }
+    *sorted = src;
+    return ok();
+}
+
+// ---------------------------------------------------------------- transpose
+
+// keys[j] = (target << 32) | source for every entry j (a warp walks 32 rows).
+__global__ void __launch_bounds__(256) transpose_keys_kernel(const uint32_t* __restrict__ offsets,
+                                                             const uint32_t* __restrict__ targets, uint32_t V,
+                                                             uint64_t* __restrict__ keys) {
+    const unsigned lane = lane_id();
+    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
+        const uint32_t count = static_cast<uint32_t>(min_u64(32, V - base));
+        uint32_t s = 0, e = 0;
+        if (lane < count) {
+            s = offsets[base + lane];
+            e = offsets[base + lane + 1];
+        }
+        for (uint32_t i = 0; i < count; ++i) {
+            const uint32_t start = __shfl_sync(kFullMask, s, i), end = __shfl_sync(kFullMask, e, i);
+            const uint64_t u = base + i;
+            for (uint32_t j = start + lane; j < end; j += 32)
+                keys[j] = (static_cast<uint64_t>(targets[j]) << 32) | u;
+        }
+    }
+}
+
+__global__ void transpose_split_kernel(const uint64_t* __restrict__ keys, uint32_t E, uint32_t* __restrict__ t_targets,
+                                       uint32_t* __restrict__ in_degree) {
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < E;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t k = keys[j];
+        t_targets[j] = static_cast<uint32_t>(k);
+        atomicAdd(in_degree + (k >> 32), 1u);
+    }
+}
+
+Error transpose_csr(DeviceImpl& dev, const uint32_t* offsets, const uint32_t* targets, uint32_t V, uint32_t E,
+                    DeviceBuffer<uint32_t>* t_offsets, DeviceBuffer<uint32_t>* t_targets) {
+    GCU_TRY(t_offsets->allocate(dev, static_cast<uint64_t>(V) + 1));
+    GCU_TRY(t_targets->allocate(dev, E));
+    GCU_CUDA(cudaMemsetAsync(t_offsets->ptr, 0, sizeof(uint32_t) * (static_cast<size_t>(V) + 1), dev.stream), "memset");
+    if (E == 0) return ok();
+    DeviceBuffer<uint64_t> keys, tmp;
+    GCU_TRY(keys.allocate(dev, E));
+    GCU_TRY(tmp.allocate(dev, E));
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned vgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
+    const unsigned egrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
+    GCU_LAUNCH(dev, "transpose_keys", transpose_keys_kernel, vgrid, 256, 0, offsets, targets, V, keys.ptr);
+    uint32_t bits = 0;
+    while (bits < 32 && (static_cast<uint64_t>(1) << bits) < V) ++bits;
+    uint64_t* sorted = nullptr;
+    // Stable sort by target only: sources stay ascending inside each in-list.
+    GCU_TRY(radix_sort_u64(dev, keys.ptr, tmp.ptr, E, 32, 32 + ((bits + 7) / 8) * 8, &sorted));
+    GCU_LAUNCH(dev, "transpose_split", transpose_split_kernel, egrid, 256, 0, sorted, E, t_targets->ptr,
+               t_offsets->ptr);
+    GCU_TRY(exclusive_scan_u32(dev, t_offsets->ptr, t_offsets->ptr, V));
+    GCU_TRY(dev.sync());  // keys/tmp are freed on return
+    return ok();
+}
+
+}  // namespace gcu

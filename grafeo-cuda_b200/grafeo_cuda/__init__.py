@@ -366,6 +366,43 @@ class GpuGraph:
             "time_seconds": float(secs.value),
         }
 
+    def _pagerank_result(self, call, copy_result: bool) -> dict:
+        n = self.num_nodes
+        ranks = np.empty(n, dtype=np.float32) if copy_result else None
+        it = C.c_uint32()
+        conv = C.c_int()
+        secs = C.c_double()
+        ptr = ranks.ctypes.data_as(C.POINTER(C.c_float)) if copy_result and n else None
+        check(call(ptr, C.byref(it), C.byref(conv), C.byref(secs)))
+        return {
+            "ranks": ranks,
+            "iterations": int(it.value),
+            "converged": bool(conv.value),
+            "time_seconds": float(secs.value),
+        }
+
+    def pagerank_directed(self, damping: float = 0.85, max_iterations: int = 100, tolerance: float = 1e-6,
+                          copy_result: bool = True) -> dict:
+        """PageRank of the directed graph whose out-edges are the CSR lists
+        (pulls over a transpose built on the device)."""
+        max_iterations = self._check_u32(max_iterations, "max_iterations")
+        return self._pagerank_result(
+            lambda *a: lib.gcu_pagerank_directed(self._h, float(damping), max_iterations, float(tolerance), *a),
+            copy_result,
+        )
+
+    def personalized_pagerank(self, seeds, damping: float = 0.85, max_iterations: int = 100,
+                              tolerance: float = 1e-6, directed: bool = False, copy_result: bool = True) -> dict:
+        """PageRank whose teleport and dangling mass go to `seeds` uniformly."""
+        max_iterations = self._check_u32(max_iterations, "max_iterations")
+        s = _u32_array(seeds, "seeds")
+        return self._pagerank_result(
+            lambda *a: lib.gcu_personalized_pagerank(
+                self._h, _ptr(s), s.size, 1 if directed else 0, float(damping), max_iterations, float(tolerance), *a
+            ),
+            copy_result,
+        )
+
     def k_truss_array(self, k: int) -> dict:
         k = self._check_u32(k, "k")
         h = C.c_void_p()

@@ -81,6 +81,35 @@ SIGNATURES = {
             C.POINTER(C.c_double),
         ],
     ),
+    "gcu_pagerank_directed": (
+        C.c_int,
+        [
+            C.c_void_p,
+            C.c_float,
+            C.c_uint32,
+            C.c_float,
+            f32p,
+            C.POINTER(C.c_uint32),
+            C.POINTER(C.c_int),
+            C.POINTER(C.c_double),
+        ],
+    ),
+    "gcu_personalized_pagerank": (
+        C.c_int,
+        [
+            C.c_void_p,
+            u32p,
+            C.c_size_t,
+            C.c_int,
+            C.c_float,
+            C.c_uint32,
+            C.c_float,
+            f32p,
+            C.POINTER(C.c_uint32),
+            C.POINTER(C.c_int),
+            C.POINTER(C.c_double),
+        ],
+    ),
     "gcu_k_truss": (
         C.c_int,
         [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_uint32), C.POINTER(C.c_double)],

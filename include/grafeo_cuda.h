@@ -178,6 +178,24 @@ GCU_API gcu_status gcu_pagerank(gcu_graph* g, float damping, uint32_t max_iterat
                                 float tolerance, float* ranks, uint32_t* iterations,
                                 int* converged, double* seconds);
 
+/* Directed PageRank. The reference can only pull over the CSR lists, which is
+ * right for symmetric graphs (pagerank.rs:10 notes that directed graphs need a
+ * transpose). Here the lists are the out-edges: the library builds the
+ * transpose on the device (stable radix sort, cached on the graph), pulls over
+ * the in-lists, takes out-degrees from the lists, and treats vertices without
+ * out-edges as dangling. Same arguments and results as gcu_pagerank. */
+GCU_API gcu_status gcu_pagerank_directed(gcu_graph* g, float damping, uint32_t max_iterations, float tolerance,
+                                         float* ranks, uint32_t* iterations, int* converged, double* seconds);
+
+/* Personalised PageRank: the teleport share and the dangling mass go to the
+ * n_seeds seed vertices (each seed 1/n_seeds, repeats add up) instead of all
+ * vertices uniformly; ranks still start at 1/N. directed = 0 pulls over the
+ * lists (symmetric graph), 1 over the transpose as in gcu_pagerank_directed.
+ * A seed >= num_nodes, or no seeds, is GCU_ERR_KERNEL. */
+GCU_API gcu_status gcu_personalized_pagerank(gcu_graph* g, const uint32_t* seeds, size_t n_seeds, int directed,
+                                             float damping, uint32_t max_iterations, float tolerance, float* ranks,
+                                             uint32_t* iterations, int* converged, double* seconds);
+
 typedef struct gcu_edge_list gcu_edge_list; /* Vec<(u32, u32)>, host memory */
 
 /* k_truss::k_truss(graph, k) (k_truss.rs:42-161). Edges (u, v) with u < v in

@@ -131,6 +131,13 @@ void orc_bfs(const uint32_t* offsets, const uint32_t* targets, uint32_t n, uint3
 void orc_pagerank(const uint32_t* offsets, const uint32_t* targets, uint32_t n, const uint32_t* out_degree,
                   double damping, uint32_t max_iterations, double tolerance, int rule, double* ranks,
                   uint32_t* iterations, int* converged) {
+    orc_pagerank_tele(offsets, targets, n, out_degree, NULL, damping, max_iterations, tolerance, rule, ranks,
+                      iterations, converged);
+}
+
+void orc_pagerank_tele(const uint32_t* offsets, const uint32_t* targets, uint32_t n, const uint32_t* out_degree,
+                       const double* tele, double damping, uint32_t max_iterations, double tolerance, int rule,
+                       double* ranks, uint32_t* iterations, int* converged) {
     *iterations = 0;
     *converged = 0;
     if (n == 0) {
@@ -159,7 +166,8 @@ void orc_pagerank(const uint32_t* offsets, const uint32_t* targets, uint32_t n, 
         for (int64_t v = 0; v < (int64_t)n; ++v) {
             double s = 0.0;
             for (uint32_t j = offsets[v]; j < offsets[v + 1]; ++j) s += contrib[targets[j]];
-            double x = base + damping * (s + spread);
+            double x = tele ? (1.0 - damping) * tele[v] + damping * (s + dangling * tele[v])
+                            : base + damping * (s + spread);
             double d = fabs(x - r[v]);
             l1 += d;
             if (d > linf) linf = d;
@@ -324,4 +332,18 @@ size_t orc_from_edge_pairs_oriented(const uint32_t* pairs, size_t n_pairs, uint3
     free(degree);
     free(keys);
     return r;
+}
+
+size_t orc_transpose(const uint32_t* offsets, const uint32_t* targets, uint32_t n, uint32_t* t_offsets,
+                     uint32_t* t_targets) {
+    const size_t E = offsets[n];
+    memset(t_offsets, 0, sizeof(uint32_t) * ((size_t)n + 1));
+    for (size_t j = 0; j < E; ++j) t_offsets[targets[j] + 1] += 1;
+    for (size_t v = 1; v <= n; ++v) t_offsets[v] += t_offsets[v - 1];
+    uint32_t* cursor = (uint32_t*)malloc(sizeof(uint32_t) * ((size_t)n + 1));
+    memcpy(cursor, t_offsets, sizeof(uint32_t) * ((size_t)n + 1));
+    for (uint32_t u = 0; u < n; ++u)
+        for (uint32_t j = offsets[u]; j < offsets[u + 1]; ++j) t_targets[cursor[targets[j]]++] = u;
+    free(cursor);
+    return E;
 }

@@ -60,6 +60,17 @@ void orc_pagerank(const uint32_t* offsets, const uint32_t* targets, uint32_t n, 
                   double damping, uint32_t max_iterations, double tolerance, int rule, double* ranks,
                   uint32_t* iterations, int* converged);
 
+/* orc_pagerank with a personalisation vector tele (NULL: uniform 1/N) that
+ * takes the teleport share and the dangling mass: r'[v] = (1-d) tele[v] +
+ * d (sum + dangling tele[v]). Ranks start at 1/N either way. */
+void orc_pagerank_tele(const uint32_t* offsets, const uint32_t* targets, uint32_t n, const uint32_t* out_degree,
+                       const double* tele, double damping, uint32_t max_iterations, double tolerance, int rule,
+                       double* ranks, uint32_t* iterations, int* converged);
+
+/* In-lists of a CSR (each ordered by source); returns the entry count. */
+size_t orc_transpose(const uint32_t* offsets, const uint32_t* targets, uint32_t n, uint32_t* t_offsets,
+                     uint32_t* t_targets);
+
 /* Synchronous peeling exactly as k_truss.rs/k_truss.cu: per round, support of
  * each live entry u -> v (v > u) is the merge count of the live lists, copied to
  * the live reverse entry; live entries below k-2 are removed; repeat until a

@@ -41,6 +41,13 @@ def _load() -> C.CDLL:
         u32p, u32p, C.c_uint32, u32p, C.c_double, C.c_uint32, C.c_double, C.c_int,
         C.POINTER(C.c_double), u32p, C.POINTER(C.c_int),
     ]
+    lib.orc_pagerank_tele.restype = None
+    lib.orc_pagerank_tele.argtypes = [
+        u32p, u32p, C.c_uint32, u32p, C.POINTER(C.c_double), C.c_double, C.c_uint32, C.c_double, C.c_int,
+        C.POINTER(C.c_double), u32p, C.POINTER(C.c_int),
+    ]
+    lib.orc_transpose.restype = C.c_size_t
+    lib.orc_transpose.argtypes = [u32p, u32p, C.c_uint32, u32p, u32p]
     lib.orc_k_truss.restype = C.c_size_t
     lib.orc_k_truss.argtypes = [u32p, u32p, C.c_uint32, C.c_uint32, u32p, u32p]
     lib.orc_from_edge_pairs.restype = C.c_size_t
@@ -95,19 +102,48 @@ def bfs(offsets, targets, source: int) -> dict:
 
 
 def pagerank(offsets, targets, damping=0.85, max_iterations=100, tolerance=1e-6, rule="l1",
-             out_degree=None) -> dict:
-    """rule 'l1': the reference GPU stopping rule; 'max': Grafeo's."""
+             out_degree=None, tele=None) -> dict:
+    """rule 'l1': the reference GPU stopping rule; 'max': Grafeo's. The CSR
+    holds the pulled (in-)lists; out_degree defaults to their lengths; tele is
+    an optional personalisation vector."""
     o, t = _u32(offsets), _u32(targets)
     n = len(o) - 1
     ranks = np.zeros(max(n, 1), dtype=np.float64)
     it = C.c_uint32()
     conv = C.c_int()
     od = None if out_degree is None else _u32(out_degree)
-    lib().orc_pagerank(
-        _p(o), _p(t), n, None if od is None else _p(od), float(damping), int(max_iterations), float(tolerance),
-        0 if rule == "l1" else 1, _p(ranks, C.c_double), C.byref(it), C.byref(conv),
+    tv = None if tele is None else np.ascontiguousarray(np.asarray(tele, dtype=np.float64))
+    lib().orc_pagerank_tele(
+        _p(o), _p(t), n, None if od is None else _p(od), None if tv is None else _p(tv, C.c_double),
+        float(damping), int(max_iterations), float(tolerance), 0 if rule == "l1" else 1, _p(ranks, C.c_double),
+        C.byref(it), C.byref(conv),
     )
     return {"ranks": ranks[:n], "iterations": int(it.value), "converged": bool(conv.value)}
+
+
+def transpose(offsets, targets):
+    o, t = _u32(offsets), _u32(targets)
+    n = len(o) - 1
+    to = np.zeros(n + 1, dtype=np.uint32)
+    tt = np.zeros(max(len(t), 1), dtype=np.uint32)
+    lib().orc_transpose(_p(o), _p(t), n, _p(to), _p(tt))
+    return to, tt[: len(t)]
+
+
+def pagerank_directed(offsets, targets, damping=0.85, max_iterations=100, tolerance=1e-6, rule="l1",
+                      tele=None) -> dict:
+    """PageRank of the directed graph whose out-edges are the CSR lists."""
+    o = _u32(offsets)
+    to, tt = transpose(offsets, targets)
+    return pagerank(to, tt, damping, max_iterations, tolerance, rule, out_degree=np.diff(o), tele=tele)
+
+
+def seed_vector(n: int, seeds) -> np.ndarray:
+    """Personalisation vector of the seeds: 1/len(seeds) each, repeats add up."""
+    p = np.zeros(n, dtype=np.float64)
+    for s in seeds:
+        p[int(s)] += 1.0 / len(seeds)
+    return p
 
 
 def k_truss(offsets, targets, k: int) -> dict:

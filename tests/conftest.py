@@ -37,6 +37,12 @@ def golden_graphs() -> list[dict]:
 
 
 @pytest.fixture(scope="session")
+def pagerank_variants() -> list[dict]:
+    with open(os.path.join(GOLDEN, "pagerank_variants.json")) as f:
+        return json.load(f)["graphs"]
+
+
+@pytest.fixture(scope="session")
 def device():
     import grafeo_cuda
 

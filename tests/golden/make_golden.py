@@ -162,7 +162,59 @@ def pins() -> dict:
     }
 
 
+def directed_csr(n: int, edges) -> tuple[list[int], list[int]]:
+    adj = [set() for _ in range(n)]
+    for a, b in edges:
+        adj[a].add(b)
+    offsets, targets = [0], []
+    for v in range(n):
+        targets.extend(sorted(adj[v]))
+        offsets.append(len(targets))
+    return offsets, targets
+
+
+def pagerank_variants() -> list[dict]:
+    """Directed PageRank (out-edges = CSR lists) and personalised PageRank,
+    networkx fixed points (tol 1e-13; dangling mass follows the teleport)."""
+    import random
+
+    out = []
+    rnd = random.Random(77)
+    cases = []
+    for i in range(12):
+        n = rnd.randint(2, 14)
+        m = rnd.randint(0, 4 * n)
+        cases.append((f"directed {i}", n, [(rnd.randrange(n), rnd.randrange(n)) for _ in range(m)]))
+    cases.append(("directed chain with a sink", 5, [(0, 1), (1, 2), (2, 3), (3, 4)]))
+    cases.append(("directed star out", 6, [(0, v) for v in range(1, 6)]))
+    for name, n, edges in cases:
+        dg = nx.DiGraph()
+        dg.add_nodes_from(range(n))
+        dg.add_edges_from(edges)
+        offsets, targets = directed_csr(n, edges)
+        pr = nx.pagerank(dg, alpha=0.85, tol=1e-13, max_iter=100000)
+        seeds = sorted({rnd.randrange(n) for _ in range(2)})
+        pers = {v: (1.0 / len(seeds) if v in seeds else 0.0) for v in range(n)}
+        ppr = nx.pagerank(dg, alpha=0.85, personalization=pers, tol=1e-13, max_iter=100000)
+        out.append({"name": name, "num_nodes": n, "directed": True, "offsets": offsets, "targets": targets,
+                    "pagerank": [pr[v] for v in range(n)], "seeds": seeds, "ppr": [ppr[v] for v in range(n)]})
+    for name, n, edges in graphs.catalog()[2:9]:
+        g = nx.Graph()
+        g.add_nodes_from(range(n))
+        g.add_edges_from(edges)
+        offsets, targets = symmetric_csr(n, edges)
+        seeds = [0, n - 1]
+        pers = {v: (0.5 if v in seeds else 0.0) for v in range(n)}
+        ppr = nx.pagerank(g, alpha=0.85, personalization=pers, tol=1e-13, max_iter=100000)
+        out.append({"name": name, "num_nodes": n, "directed": False, "offsets": offsets, "targets": targets,
+                    "seeds": seeds, "ppr": [ppr[v] for v in range(n)]})
+    return out
+
+
 def main() -> None:
+    with open(os.path.join(HERE, "pagerank_variants.json"), "w") as f:
+        json.dump({"generator": "networkx " + nx.__version__, "graphs": pagerank_variants()}, f,
+                  separators=(",", ":"))
     recs = [record(name, n, e) for name, n, e in graphs.catalog()]
     n, e = graphs.messy(True, True)
     recs.append(record("messy", n, e))

@@ -133,6 +133,28 @@ def test_oracle_oriented_builder_rules(seed):
     assert O.triangle_count_oriented(o, t) == brute
 
 
+def test_oracle_directed_and_personalized_pagerank_match_networkx(pagerank_variants):
+    for g in pagerank_variants:
+        o, t = csr(g)
+        n = g["num_nodes"]
+        tele = O.seed_vector(n, g["seeds"])
+        if g["directed"]:
+            r = O.pagerank_directed(o, t, 0.85, 100000, 1e-15, rule="max")
+            assert r["converged"]
+            np.testing.assert_allclose(r["ranks"], g["pagerank"], atol=1e-10, rtol=0, err_msg=g["name"])
+            r = O.pagerank_directed(o, t, 0.85, 100000, 1e-15, rule="max", tele=tele)
+        else:
+            r = O.pagerank(o, t, 0.85, 100000, 1e-15, rule="max", tele=tele)
+        assert r["converged"]
+        np.testing.assert_allclose(r["ranks"], g["ppr"], atol=1e-10, rtol=0, err_msg=g["name"])
+        assert abs(r["ranks"].sum() - 1.0) < 1e-12
+
+
+def test_oracle_transpose():
+    o, t = O.transpose([0, 2, 3, 3, 4], [1, 3, 2, 0])
+    assert o.tolist() == [0, 1, 2, 3, 4] and t.tolist() == [3, 0, 1, 0]
+
+
 def test_oracle_k_truss_round_semantics_on_self_loops():
     """A self-loop inflates first-round support (the reference merges raw lists,
     kernels/k_truss.cu:59-92); the fixpoint is still the maximal k-truss."""
