@@ -207,6 +207,8 @@ Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reac
 Error pagerank(GraphImpl& g, float damping, uint32_t max_iterations, float tolerance,
                float* host_ranks, uint32_t* iterations, bool* converged);
 Error k_truss(GraphImpl& g, uint32_t k, std::vector<uint32_t>* edges, uint32_t* iterations);
+// Trussness of every CSR entry's edge (host_truss may be NULL), symmetric CSR.
+Error truss_decomposition(GraphImpl& g, uint32_t* host_truss, uint32_t* max_truss, uint32_t* rounds);
 
 // Exclusive scan of u32 counts into u32 offsets (out has n + 1 entries);
 // returns the total through the device (out[n]).

@@ -189,12 +189,14 @@ __global__ void kt_loops_kernel(const uint32_t* __restrict__ targets, const uint
 }
 
 // Round r: every alive u < v entry whose support is below the threshold is
-// removed (state = r) and listed. In round 1 a self-loop at either end adds
-// one to the support, as the reference's merge of the raw lists does.
+// removed (state = r) and listed. With `loop` in round 1 a self-loop at either
+// end adds one to the support, as the reference's merge of the raw lists
+// does. With `truss`, every removed entry also gets truss_value there.
 __global__ void kt_round_filter_kernel(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ src,
                                        const uint8_t* __restrict__ loop, const uint32_t* __restrict__ support,
                                        uint32_t* __restrict__ state, uint32_t E, uint32_t threshold, uint32_t round,
-                                       uint32_t* __restrict__ removed, uint32_t* __restrict__ removed_count) {
+                                       uint32_t* __restrict__ removed, uint32_t* __restrict__ removed_count,
+                                       uint32_t* __restrict__ truss, uint32_t truss_value) {
     const unsigned lane = lane_id();
     for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~31ull; base < E;
          base += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -204,8 +206,9 @@ __global__ void kt_round_filter_kernel(const uint32_t* __restrict__ targets, con
             const uint32_t u = src[j], v = targets[j];
             if (v > u) {
                 uint32_t s = support[j];
-                if (round == 1) s += loop[u] + loop[v];
+                if (loop && round == 1) s += loop[u] + loop[v];
                 take = s < threshold;
+                if (take && truss) truss[j] = truss_value;
             }
         }
         const unsigned mask = __ballot_sync(kFullMask, take);
@@ -323,6 +326,19 @@ static Error k_truss_general(GraphImpl& g, uint32_t k, const uint32_t* src, cons
     return emit_edges(dev, g, src, LiveFlag{live.ptr}, support.ptr, pos.ptr, edges);
 }
 
+// support[j] += triangles of the undirected edge whose u < v entry is j,
+// counted once on the degree DAG (symmetric CSR).
+static Error triangle_support(GraphImpl& g, const uint32_t* rev, uint32_t* support) {
+    DeviceBuffer<uint32_t> dag_offsets, dag_targets, dag_eid;
+    uint32_t m = 0;
+    GCU_TRY(build_dag(g, true, rev, &dag_offsets, &dag_targets, &dag_eid, &m));
+    if (m > 0) {
+        GCU_TRY(run_wedges(*g.dev, dag_offsets.ptr, dag_targets.ptr, g.num_nodes, 2,
+                           SupportSink{dag_eid.ptr, support}, "kt"));
+    }
+    return ok();
+}
+
 // Symmetric CSR: per-edge triangle counts from the DAG, then incremental
 // peeling. Every round removes exactly the entries the reference's round
 // removes, so the edge list and the round count are the same.
@@ -346,16 +362,7 @@ static Error k_truss_symmetric(GraphImpl& g, uint32_t k, const uint32_t* src, co
     const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
     GCU_LAUNCH(dev, "kt_loops", kt_loops_kernel, edge_grid, 256, 0, g.targets.ptr, src, E, loop.ptr, scratch.ptr + 1);
 
-    // Support = triangles per undirected edge, counted on the degree DAG.
-    {
-        DeviceBuffer<uint32_t> dag_offsets, dag_targets, dag_eid;
-        uint32_t m = 0;
-        GCU_TRY(build_dag(g, true, rev, &dag_offsets, &dag_targets, &dag_eid, &m));
-        if (m > 0) {
-            GCU_TRY(run_wedges(dev, dag_offsets.ptr, dag_targets.ptr, V, 2, SupportSink{dag_eid.ptr, support.ptr},
-                               "kt"));
-        }
-    }
+    GCU_TRY(triangle_support(g, rev, support.ptr));
     uint32_t loops = 0;
     GCU_CUDA(cudaMemcpyAsync(&loops, scratch.ptr + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
     GCU_TRY(dev.sync());
@@ -364,7 +371,7 @@ static Error k_truss_symmetric(GraphImpl& g, uint32_t k, const uint32_t* src, co
     while (true) {
         GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
         GCU_LAUNCH(dev, "kt_round_filter", kt_round_filter_kernel, edge_grid, 256, 0, g.targets.ptr, src, loop.ptr,
-                   support.ptr, state.ptr, E, threshold, round, removed.ptr, scratch.ptr);
+                   support.ptr, state.ptr, E, threshold, round, removed.ptr, scratch.ptr, nullptr, 0u);
         uint32_t n = 0;
         GCU_CUDA(cudaMemcpyAsync(&n, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
         GCU_TRY(dev.sync());
@@ -404,6 +411,99 @@ Error k_truss(GraphImpl& g, uint32_t k, std::vector<uint32_t>* edges, uint32_t* 
                rev.ptr);
     if (symmetric) return k_truss_symmetric(g, k, src.ptr, rev.ptr, edges, iterations);
     return k_truss_general(g, k, src.ptr, rev.ptr, edges, iterations);
+}
+
+// ---------------------------------------------------------------- truss decomposition
+
+// Spreads the u < v entries' trussness to every entry: the reverse entry gets
+// the same value, self-loops 0.
+__global__ void kt_truss_spread_kernel(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ src,
+                                       const uint32_t* __restrict__ rev, const uint32_t* __restrict__ truss,
+                                       uint32_t E, uint32_t* __restrict__ out) {
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < E;
+         j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t u = src[j], v = targets[j];
+        out[j] = u == v ? 0u : truss[u < v ? j : rev[j]];
+    }
+}
+
+// Trussness of every edge of a symmetric CSR: the peeling of k_truss_symmetric
+// continued level by level without restarting. At level k the rounds remove
+// every alive edge with fewer than k - 2 alive triangles until none is left
+// below; the edges removed at level k have trussness k - 1. Self-loops take no
+// part (they are in no k-truss for k >= 3).
+Error truss_decomposition(GraphImpl& g, uint32_t* host_truss, uint32_t* max_truss, uint32_t* rounds) {
+    *max_truss = 0;
+    *rounds = 0;
+    const uint32_t E = g.num_edges, V = g.num_nodes;
+    if (E == 0) return ok();
+    DeviceImpl& dev = *g.dev;
+    bool symmetric = false;
+    GCU_TRY(graph_symmetry(g, &symmetric));
+    if (!symmetric) return kernel_error("truss decomposition needs a symmetric CSR (every u -> v with its v -> u)");
+    DeviceBuffer<uint32_t> src, rev, support, state, removed, truss, scratch;
+    GCU_TRY(src.allocate(dev, E));
+    GCU_TRY(rev.allocate(dev, E));
+    GCU_TRY(support.allocate(dev, E));
+    GCU_TRY(state.allocate(dev, E));
+    GCU_TRY(removed.allocate(dev, E));
+    GCU_TRY(truss.allocate(dev, E));
+    GCU_TRY(scratch.allocate(dev, 2));
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned row_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
+    const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
+    GCU_LAUNCH(dev, "kt_rows", kt_rows_kernel, row_grid, 256, 0, g.offsets.ptr, V, src.ptr);
+    GCU_LAUNCH(dev, "kt_reverse", kt_reverse_kernel, edge_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src.ptr, E,
+               rev.ptr);
+    GCU_CUDA(cudaMemsetAsync(support.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(state.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(truss.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
+    GCU_TRY(triangle_support(g, rev.ptr, support.ptr));
+    // Undirected edges alive: in a symmetric CSR every edge but a self-loop
+    // has two entries, so there are (E - self-loop entries) / 2 of them.
+    DeviceBuffer<uint8_t> loop;
+    GCU_TRY(loop.allocate(dev, V));
+    GCU_CUDA(cudaMemsetAsync(loop.ptr, 0, V, dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, 2 * sizeof(uint32_t), dev.stream), "memset");
+    GCU_LAUNCH(dev, "kt_loops", kt_loops_kernel, edge_grid, 256, 0, g.targets.ptr, src.ptr, E, loop.ptr,
+               scratch.ptr + 1);
+    uint32_t loops = 0;
+    GCU_CUDA(cudaMemcpyAsync(&loops, scratch.ptr + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+    GCU_TRY(dev.sync());
+    uint64_t alive = (static_cast<uint64_t>(E) - loops) / 2;
+    uint32_t round = 0, k = 3, top = alive > 0 ? 2 : 0;
+    while (alive > 0) {
+        round += 1;
+        GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
+        GCU_LAUNCH(dev, "kt_round_filter", kt_round_filter_kernel, edge_grid, 256, 0, g.targets.ptr, src.ptr,
+                   static_cast<const uint8_t*>(nullptr), support.ptr, state.ptr, E, k - 2, round, removed.ptr,
+                   scratch.ptr, truss.ptr, k - 1);
+        uint32_t n = 0;
+        GCU_CUDA(cudaMemcpyAsync(&n, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+        GCU_TRY(dev.sync());
+        if (n == 0) {
+            // Every alive edge has at least k - 2 alive triangles: it is in the k-truss.
+            top = k;
+            k += 1;
+            continue;
+        }
+        alive -= n;
+        const unsigned peel_grid =
+            static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(static_cast<uint64_t>(n) * 32, 256), cap));
+        GCU_LAUNCH(dev, "kt_peel", kt_peel_kernel, peel_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src.ptr, rev.ptr,
+                   state.ptr, support.ptr, removed.ptr, scratch.ptr, round);
+    }
+    *max_truss = top;
+    *rounds = round;
+    if (host_truss) {
+        GCU_LAUNCH(dev, "kt_truss_spread", kt_truss_spread_kernel, edge_grid, 256, 0, g.targets.ptr, src.ptr, rev.ptr,
+                   truss.ptr, E, support.ptr);
+        GCU_CUDA(cudaMemcpyAsync(host_truss, support.ptr, sizeof(uint32_t) * static_cast<size_t>(E),
+                                 cudaMemcpyDeviceToHost, dev.stream),
+                 "copy trussness to host");
+        GCU_TRY(dev.sync());
+    }
+    return ok();
 }
 
 }  // namespace gcu

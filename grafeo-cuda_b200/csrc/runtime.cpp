@@ -522,6 +522,22 @@ GCU_API gcu_status gcu_k_truss(gcu_graph* g, uint32_t k, gcu_edge_list** edges, 
     return succeed();
 }
 
+GCU_API gcu_status gcu_truss_decomposition(gcu_graph* g, uint32_t* trussness, uint32_t* max_trussness,
+                                           uint32_t* rounds, double* seconds) {
+    WallTimer wall;
+    if (!g) return fail(kernel_error("graph is NULL"));
+    GraphImpl& gi = *g->impl;
+    std::lock_guard<std::mutex> lock(gi.mu);
+    Error e = gi.dev->activate();
+    uint32_t top = 0, r = 0;
+    if (e.ok()) e = truss_decomposition(gi, trussness, &top, &r);
+    if (!e.ok()) return fail(e);
+    if (max_trussness) *max_trussness = top;
+    if (rounds) *rounds = r;
+    if (seconds) *seconds = wall.seconds();
+    return succeed();
+}
+
 GCU_API size_t gcu_edge_list_len(const gcu_edge_list* list) { return list ? list->data.size() / 2 : 0; }
 GCU_API const uint32_t* gcu_edge_list_data(const gcu_edge_list* list) {
     return list && !list->data.empty() ? list->data.data() : nullptr;

@@ -403,6 +403,19 @@ class GpuGraph:
             copy_result,
         )
 
+    def truss_decomposition(self, copy_result: bool = True) -> dict:
+        """Trussness of every CSR entry's edge (symmetric CSR): the largest k
+        whose k-truss holds the edge (2: in no triangle, 0: self-loop)."""
+        n = self.num_edges
+        truss = np.empty(n, dtype=np.uint32) if copy_result else None
+        top = C.c_uint32()
+        rounds = C.c_uint32()
+        secs = C.c_double()
+        ptr = truss.ctypes.data_as(C.POINTER(C.c_uint32)) if copy_result and n else None
+        check(lib.gcu_truss_decomposition(self._h, ptr, C.byref(top), C.byref(rounds), C.byref(secs)))
+        return {"trussness": truss, "max_trussness": int(top.value), "rounds": int(rounds.value),
+                "time_seconds": float(secs.value)}
+
     def k_truss_array(self, k: int) -> dict:
         k = self._check_u32(k, "k")
         h = C.c_void_p()

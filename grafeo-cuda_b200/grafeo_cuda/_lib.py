@@ -114,6 +114,10 @@ SIGNATURES = {
         C.c_int,
         [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_uint32), C.POINTER(C.c_double)],
     ),
+    "gcu_truss_decomposition": (
+        C.c_int,
+        [C.c_void_p, u32p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_double)],
+    ),
     "gcu_edge_list_len": (C.c_size_t, [C.c_void_p]),
     "gcu_edge_list_data": (u32p, [C.c_void_p]),
     "gcu_edge_list_free": (None, [C.c_void_p]),

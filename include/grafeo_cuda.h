@@ -202,6 +202,17 @@ typedef struct gcu_edge_list gcu_edge_list; /* Vec<(u32, u32)>, host memory */
  * CSR order. k < 3 is GCU_ERR_KERNEL. */
 GCU_API gcu_status gcu_k_truss(gcu_graph* g, uint32_t k, gcu_edge_list** edges,
                                uint32_t* iterations, double* seconds);
+/* Truss decomposition. No single reference call: the reference's tests sweep
+ * k_truss for k = 3..8 (tests/correctness.rs:305-326). For every CSR entry
+ * u -> v, trussness[j] = the largest k whose k-truss contains the edge {u, v}
+ * (2 for an edge in no triangle, 0 for a self-loop entry), so that
+ * gcu_k_truss(g, k) returns exactly the entries with u < v and trussness >= k.
+ * trussness (num_edges u32) may be NULL. *max_trussness = the largest k with a
+ * non-empty k-truss (0 without edges); *rounds = peeling rounds run.
+ * Symmetric CSR only (GCU_ERR_KERNEL otherwise). */
+GCU_API gcu_status gcu_truss_decomposition(gcu_graph* g, uint32_t* trussness, uint32_t* max_trussness,
+                                           uint32_t* rounds, double* seconds);
+
 GCU_API size_t gcu_edge_list_len(const gcu_edge_list* list);
 /* 2 * len values: u0, v0, u1, v1, ... */
 GCU_API const uint32_t* gcu_edge_list_data(const gcu_edge_list* list);

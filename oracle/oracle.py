@@ -155,6 +155,28 @@ def k_truss(offsets, targets, k: int) -> dict:
     return {"edges": out[: 2 * m].reshape(m, 2), "iterations": int(it.value)}
 
 
+def truss_decomposition(offsets, targets) -> dict:
+    """Trussness per CSR entry from the definition: the largest k whose
+    k-truss (k_truss above, k = 3, 4, ...) holds the edge; 2 for the other
+    edges, 0 for self-loops. Symmetric CSR."""
+    o, t = _u32(offsets), _u32(targets)
+    n = len(o) - 1
+    src = np.repeat(np.arange(n, dtype=np.uint32), np.diff(o))
+    truss = np.where(src == t, 0, 2).astype(np.uint32)
+    key = (src.astype(np.uint64) << np.uint64(32)) | t.astype(np.uint64)  # sorted: CSR order
+    k, top = 3, (2 if np.any(src != t) else 0)
+    while True:
+        edges = k_truss(o, t, k)["edges"]
+        if len(edges) == 0:
+            break
+        u, v = edges[:, 0].astype(np.uint64), edges[:, 1].astype(np.uint64)
+        for a, b in ((u, v), (v, u)):
+            truss[np.searchsorted(key, (a << np.uint64(32)) | b)] = k
+        top = k
+        k += 1
+    return {"trussness": truss, "max_trussness": top}
+
+
 def from_edge_pairs(edges, num_nodes: int, symmetric: bool):
     p = _u32(edges).reshape(-1)
     offsets = np.zeros(num_nodes + 1, dtype=np.uint32)

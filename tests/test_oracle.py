@@ -150,6 +150,18 @@ def test_oracle_directed_and_personalized_pagerank_match_networkx(pagerank_varia
         assert abs(r["ranks"].sum() - 1.0) < 1e-12
 
 
+def test_oracle_truss_decomposition_matches_networkx_trusses(golden_graphs):
+    for g in golden_graphs:
+        o, t = csr(g)
+        r = O.truss_decomposition(o, t)
+        src = np.repeat(np.arange(g["num_nodes"]), np.diff(o))
+        upper = [(int(a), int(b), int(x)) for a, b, x in zip(src, t, r["trussness"]) if a < b]
+        for k in range(3, 9):
+            got = sorted((a, b) for a, b, x in upper if x >= k)
+            assert got == [tuple(e) for e in g["k_truss"][str(k)]], (g["name"], k)
+        assert all(x == 0 for a, b, x in zip(src, t, r["trussness"]) if a == b)
+
+
 def test_oracle_transpose():
     o, t = O.transpose([0, 2, 3, 3, 4], [1, 3, 2, 0])
     assert o.tolist() == [0, 1, 2, 3, 4] and t.tolist() == [3, 0, 1, 0]
