@@ -233,6 +233,30 @@ Error pagerank_ex(GraphImpl& g, bool directed, const float* tele, float damping,
 void destroy_pagerank_plan(PageRankPlan* p);
 void destroy_bfs_work(BfsWork* w);
 
+// ---------------------------------------------------------------- device CSR build
+
+// Edge pairs (host, interleaved src/dst) -> the graph's CSR, built on the
+// device. mode 0: directed (from_edge_pairs, symmetric = false), 1: symmetric
+// (from_edge_pairs, symmetric = true), 2: degree-oriented
+// (from_edge_pairs_oriented).
+Error build_graph_from_pairs(DeviceImpl& dev, const uint32_t* host_pairs, uint64_t n_pairs, uint32_t num_nodes,
+                             int mode, GraphImpl& g);
+
+// Synthetic graph drawn on the device (symmetric, loop-free, deduplicated).
+struct GeneratorSpec {
+    enum Kind { kRmat, kErdosRenyi, kGrid, kWattsStrogatz, kGeometric } kind = kRmat;
+    uint64_t seed = 0;
+    uint32_t scale = 0, edge_factor = 0;  // R-MAT
+    double a = 0, b = 0, c = 0;           // R-MAT quadrant probabilities
+    uint32_t n = 0;                       // Erdos-Renyi, Watts-Strogatz, geometric vertices
+    uint64_t pairs = 0;                   // Erdos-Renyi drawn pairs
+    uint32_t width = 0, height = 0;       // grid
+    uint32_t k = 0;                       // Watts-Strogatz lattice degree (even)
+    double p = 0;                         // grid drop / Watts-Strogatz rewire probability
+    double avg_degree = 0;                // geometric
+};
+Error generate_graph(DeviceImpl& dev, const GeneratorSpec& spec, GraphImpl& g);
+
 }  // namespace gcu
 
 // Launch helper: counts the launch, brackets it with events when per-kernel

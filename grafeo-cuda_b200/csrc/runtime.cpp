@@ -392,6 +392,120 @@ GCU_API uint32_t gcu_graph_num_nodes(const gcu_graph* g) { return g ? g->impl->n
 GCU_API uint32_t gcu_graph_num_edges(const gcu_graph* g) { return g ? g->impl->num_edges : 0; }
 GCU_API void gcu_graph_destroy(gcu_graph* g) { delete g; }
 
+GCU_API gcu_status gcu_graph_copy_csr(const gcu_graph* g, uint32_t* offsets, uint32_t* targets) {
+    if (!g || !offsets || (g->impl->num_edges && !targets)) return fail(kernel_error("gcu_graph_copy_csr: NULL argument"));
+    GraphImpl& gi = *g->impl;
+    DeviceImpl& d = *gi.dev;
+    Error e = d.activate();
+    if (!e.ok()) return fail(e);
+    cudaError_t c = cudaMemcpyAsync(offsets, gi.offsets.ptr, 4 * (static_cast<size_t>(gi.num_nodes) + 1),
+                                    cudaMemcpyDeviceToHost, d.stream);
+    if (c == cudaSuccess && gi.num_edges)
+        c = cudaMemcpyAsync(targets, gi.targets.ptr, 4 * static_cast<size_t>(gi.num_edges), cudaMemcpyDeviceToHost,
+                            d.stream);
+    if (c != cudaSuccess) return fail(driver_error(c, "copy CSR to host"));
+    e = d.sync();
+    return e.ok() ? succeed() : fail(e);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Runs a device CSR build into a new graph handle.
+template <typename Build>
+gcu_status new_device_graph(gcu_device* dev, gcu_graph** out, Build&& build) {
+    if (!out) return fail(kernel_error("out is NULL"));
+    *out = nullptr;
+    if (!dev) return fail(kernel_error("device is NULL"));
+    auto g = std::make_unique<GraphImpl>();
+    g->dev = dev->impl;
+    Error e = g->dev->activate();
+    if (e.ok()) e = build(*g->dev, *g);
+    if (!e.ok()) return fail(e);
+    *out = new gcu_graph{std::move(g)};
+    return succeed();
+}
+
+}  // namespace
+
+extern "C" {
+
+GCU_API gcu_status gcu_graph_from_edge_pairs(gcu_device* dev, const uint32_t* pairs, size_t n_pairs,
+                                             uint32_t num_nodes, int symmetric, gcu_graph** out) {
+    if (n_pairs && !pairs) return fail(kernel_error("pairs is NULL"));
+    return new_device_graph(dev, out, [&](DeviceImpl& d, GraphImpl& g) {
+        return build_graph_from_pairs(d, pairs, n_pairs, num_nodes, symmetric ? 1 : 0, g);
+    });
+}
+
+GCU_API gcu_status gcu_graph_from_edge_pairs_oriented(gcu_device* dev, const uint32_t* pairs, size_t n_pairs,
+                                                      uint32_t num_nodes, gcu_graph** out) {
+    if (n_pairs && !pairs) return fail(kernel_error("pairs is NULL"));
+    return new_device_graph(dev, out, [&](DeviceImpl& d, GraphImpl& g) {
+        return build_graph_from_pairs(d, pairs, n_pairs, num_nodes, 2, g);
+    });
+}
+
+static gcu_status generate(gcu_device* dev, const GeneratorSpec& spec, gcu_graph** out) {
+    return new_device_graph(dev, out, [&](DeviceImpl& d, GraphImpl& g) { return generate_graph(d, spec, g); });
+}
+
+GCU_API gcu_status gcu_graph_generate_rmat(gcu_device* dev, uint32_t scale, uint32_t edge_factor, double a, double b,
+                                           double c, uint64_t seed, gcu_graph** out) {
+    GeneratorSpec s;
+    s.kind = GeneratorSpec::kRmat;
+    s.scale = scale;
+    s.edge_factor = edge_factor;
+    s.a = a;
+    s.b = b;
+    s.c = c;
+    s.seed = seed;
+    return generate(dev, s, out);
+}
+
+GCU_API gcu_status gcu_graph_generate_erdos_renyi(gcu_device* dev, uint32_t num_nodes, uint64_t num_pairs,
+                                                  uint64_t seed, gcu_graph** out) {
+    GeneratorSpec s;
+    s.kind = GeneratorSpec::kErdosRenyi;
+    s.n = num_nodes;
+    s.pairs = num_pairs;
+    s.seed = seed;
+    return generate(dev, s, out);
+}
+
+GCU_API gcu_status gcu_graph_generate_grid(gcu_device* dev, uint32_t width, uint32_t height, double drop,
+                                           uint64_t seed, gcu_graph** out) {
+    GeneratorSpec s;
+    s.kind = GeneratorSpec::kGrid;
+    s.width = width;
+    s.height = height;
+    s.p = drop;
+    s.seed = seed;
+    return generate(dev, s, out);
+}
+
+GCU_API gcu_status gcu_graph_generate_watts_strogatz(gcu_device* dev, uint32_t num_nodes, uint32_t k, double p,
+                                                     uint64_t seed, gcu_graph** out) {
+    GeneratorSpec s;
+    s.kind = GeneratorSpec::kWattsStrogatz;
+    s.n = num_nodes;
+    s.k = k;
+    s.p = p;
+    s.seed = seed;
+    return generate(dev, s, out);
+}
+
+GCU_API gcu_status gcu_graph_generate_geometric(gcu_device* dev, uint32_t num_nodes, double avg_degree, uint64_t seed,
+                                                gcu_graph** out) {
+    GeneratorSpec s;
+    s.kind = GeneratorSpec::kGeometric;
+    s.n = num_nodes;
+    s.avg_degree = avg_degree;
+    s.seed = seed;
+    return generate(dev, s, out);
+}
+
 GCU_API gcu_status gcu_triangle_count(gcu_graph* g, uint64_t* total, double* seconds) {
     WallTimer wall;
     if (!g) return fail(kernel_error("graph is NULL"));

@@ -280,6 +280,59 @@ class GpuGraph:
             csr.validate()
         return GpuGraph.from_csr(csr.offsets, csr.targets, device)
 
+    @staticmethod
+    def _built(call, device: GpuDevice, *args) -> "GpuGraph":
+        h = C.c_void_p()
+        check(call(device._h, *args, C.byref(h)))
+        return GpuGraph(h, device)
+
+    @staticmethod
+    def from_edge_pairs(edges, num_nodes: int, symmetric: bool, device: GpuDevice) -> "GpuGraph":
+        """from_edge_pairs + from_csr_arrays (csr_export.rs:202-239), sorted and
+        deduplicated on the device."""
+        p = _pairs(edges)
+        return GpuGraph._built(lib.gcu_graph_from_edge_pairs, device, _ptr(p), p.shape[0], int(num_nodes),
+                               1 if symmetric else 0)
+
+    @staticmethod
+    def from_edge_pairs_oriented(edges, num_nodes: int, device: GpuDevice) -> "GpuGraph":
+        """from_edge_pairs_oriented (csr_export.rs:299-350) on the device."""
+        p = _pairs(edges)
+        return GpuGraph._built(lib.gcu_graph_from_edge_pairs_oriented, device, _ptr(p), p.shape[0], int(num_nodes))
+
+    @staticmethod
+    def generate_rmat(device: GpuDevice, scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19,
+                      c: float = 0.19, seed: int = 1) -> "GpuGraph":
+        """generate_rmat drawn on the device (the same CSR)."""
+        return GpuGraph._built(lib.gcu_graph_generate_rmat, device, int(scale), int(edge_factor), float(a), float(b),
+                               float(c), int(seed))
+
+    @staticmethod
+    def generate_erdos_renyi(device: GpuDevice, num_nodes: int, num_pairs: int, seed: int = 3) -> "GpuGraph":
+        return GpuGraph._built(lib.gcu_graph_generate_erdos_renyi, device, int(num_nodes), int(num_pairs), int(seed))
+
+    @staticmethod
+    def generate_grid(device: GpuDevice, width: int, height: int, drop: float = 0.05, seed: int = 0) -> "GpuGraph":
+        return GpuGraph._built(lib.gcu_graph_generate_grid, device, int(width), int(height), float(drop), int(seed))
+
+    @staticmethod
+    def generate_watts_strogatz(device: GpuDevice, num_nodes: int, k: int = 10, p: float = 0.1,
+                                seed: int = 0) -> "GpuGraph":
+        return GpuGraph._built(lib.gcu_graph_generate_watts_strogatz, device, int(num_nodes), int(k), float(p),
+                               int(seed))
+
+    @staticmethod
+    def generate_geometric(device: GpuDevice, num_nodes: int, avg_degree: float, seed: int = 0) -> "GpuGraph":
+        return GpuGraph._built(lib.gcu_graph_generate_geometric, device, int(num_nodes), float(avg_degree),
+                               int(seed))
+
+    def to_csr(self) -> CsrArrays:
+        """The device CSR copied back to host arrays."""
+        o = np.empty(self.num_nodes + 1, dtype=np.uint32)
+        t = np.empty(max(self.num_edges, 1), dtype=np.uint32)
+        check(lib.gcu_graph_copy_csr(self._h, _ptr(o), _ptr(t)))
+        return CsrArrays(o, t[: self.num_edges], self.num_nodes, self.num_edges)
+
     @property
     def num_nodes(self) -> int:
         return int(lib.gcu_graph_num_nodes(self._h))

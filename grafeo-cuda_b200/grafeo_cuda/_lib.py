@@ -58,6 +58,35 @@ SIGNATURES = {
     "gcu_graph_num_nodes": (C.c_uint32, [C.c_void_p]),
     "gcu_graph_num_edges": (C.c_uint32, [C.c_void_p]),
     "gcu_graph_destroy": (None, [C.c_void_p]),
+    "gcu_graph_copy_csr": (C.c_int, [C.c_void_p, u32p, u32p]),
+    "gcu_graph_from_edge_pairs": (
+        C.c_int,
+        [C.c_void_p, u32p, C.c_size_t, C.c_uint32, C.c_int, C.POINTER(C.c_void_p)],
+    ),
+    "gcu_graph_from_edge_pairs_oriented": (
+        C.c_int,
+        [C.c_void_p, u32p, C.c_size_t, C.c_uint32, C.POINTER(C.c_void_p)],
+    ),
+    "gcu_graph_generate_rmat": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64, C.POINTER(C.c_void_p)],
+    ),
+    "gcu_graph_generate_erdos_renyi": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.POINTER(C.c_void_p)],
+    ),
+    "gcu_graph_generate_grid": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, C.c_uint32, C.c_double, C.c_uint64, C.POINTER(C.c_void_p)],
+    ),
+    "gcu_graph_generate_watts_strogatz": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, C.c_uint32, C.c_double, C.c_uint64, C.POINTER(C.c_void_p)],
+    ),
+    "gcu_graph_generate_geometric": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, C.c_double, C.c_uint64, C.POINTER(C.c_void_p)],
+    ),
     "gcu_triangle_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "gcu_triangle_count_oriented": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "gcu_triangle_count_oriented_noalloc": (

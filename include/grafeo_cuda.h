@@ -136,6 +136,49 @@ GCU_API uint32_t gcu_graph_num_nodes(const gcu_graph* g);
 GCU_API uint32_t gcu_graph_num_edges(const gcu_graph* g);
 GCU_API void gcu_graph_destroy(gcu_graph* g);
 
+/* Copies the device CSR back: offsets gets num_nodes + 1 entries, targets
+ * num_edges (GpuGraph's public offsets/targets fields, gpu_graph.rs:17-19,
+ * read back with the reference's dtoh copies). */
+GCU_API gcu_status gcu_graph_copy_csr(const gcu_graph* g, uint32_t* offsets, uint32_t* targets);
+
+/* ---- device CSR construction (the step before the path) ---- */
+
+/* from_edge_pairs(pairs, num_nodes, symmetric) followed by
+ * GpuGraph::from_csr_arrays (csr_export.rs:202-239, gpu_graph.rs:46-60), with
+ * the sort and deduplication done on the device: `pairs` holds n_pairs
+ * interleaved (src, dst) u32 values in host memory. Same CSR and the same
+ * errors (GCU_ERR_EXPORT for a node >= num_nodes; GCU_ERR_INVALID_CSR for a
+ * directed target >= num_nodes, which the host builder lets through and
+ * validate_csr rejects). At most 2^32 - 2 entries before deduplication. */
+GCU_API gcu_status gcu_graph_from_edge_pairs(gcu_device* dev, const uint32_t* pairs, size_t n_pairs,
+                                             uint32_t num_nodes, int symmetric, gcu_graph** out);
+/* from_edge_pairs_oriented (csr_export.rs:299-350) on the device. */
+GCU_API gcu_status gcu_graph_from_edge_pairs_oriented(gcu_device* dev, const uint32_t* pairs,
+                                                      size_t n_pairs, uint32_t num_nodes,
+                                                      gcu_graph** out);
+
+/* Synthetic symmetric graphs generated on the device (loop-free, deduplicated,
+ * sorted). R-MAT and Erdos-Renyi draw exactly the pairs of gcu_generate_rmat /
+ * gcu_generate_erdos_renyi, so the CSR equals theirs. No reference
+ * counterpart: they stand in for the Graph500/GraphChallenge inputs. */
+GCU_API gcu_status gcu_graph_generate_rmat(gcu_device* dev, uint32_t scale, uint32_t edge_factor,
+                                           double a, double b, double c, uint64_t seed,
+                                           gcu_graph** out);
+GCU_API gcu_status gcu_graph_generate_erdos_renyi(gcu_device* dev, uint32_t num_nodes,
+                                                  uint64_t num_pairs, uint64_t seed, gcu_graph** out);
+/* width x height grid (vertex y * width + x); every lattice edge dropped with
+ * probability `drop`. */
+GCU_API gcu_status gcu_graph_generate_grid(gcu_device* dev, uint32_t width, uint32_t height,
+                                           double drop, uint64_t seed, gcu_graph** out);
+/* Watts-Strogatz: ring lattice of even degree k, each lattice edge (u, u + j)
+ * rewired to (u, w), w uniform, with probability p. */
+GCU_API gcu_status gcu_graph_generate_watts_strogatz(gcu_device* dev, uint32_t num_nodes, uint32_t k,
+                                                     double p, uint64_t seed, gcu_graph** out);
+/* Random geometric graph: num_nodes uniform points in the unit square, an edge
+ * between points at distance <= r, (num_nodes - 1) * pi * r^2 = avg_degree. */
+GCU_API gcu_status gcu_graph_generate_geometric(gcu_device* dev, uint32_t num_nodes, double avg_degree,
+                                                uint64_t seed, gcu_graph** out);
+
 /* ---- algorithms: crates/grafeo-cuda-algos/src ---- */
 
 /* triangle_counting::triangle_count (triangle_counting.rs:40-152): total

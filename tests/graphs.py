@@ -104,3 +104,86 @@ def wide_frontier(width: int = 500_000, depth: int = 4):
 
 K4_CSR = ([0, 3, 6, 9, 12], [1, 2, 3, 0, 2, 3, 0, 1, 3, 0, 1, 2])
 PATH5_CSR = ([0, 1, 3, 5, 7, 8], [1, 0, 2, 1, 3, 2, 4, 3])
+
+
+# ---------------------------------------------------------------- generator restatements
+# numpy restatements of the device generators (csrc/build_csr.cu), used to
+# check them pair for pair: SplitMix64 stream value n of `state` is
+# mix(state + (n + 1) * gamma), state = mix(seed + gamma).
+
+_C1, _C2 = np.uint64(0xBF58476D1CE4E5B9), np.uint64(0x94D049BB133111EB)
+_GAMMA = np.uint64(0x9E3779B97F4A7C15)
+
+
+def _mix(z: np.ndarray) -> np.ndarray:
+    with np.errstate(over="ignore"):
+        z = (z ^ (z >> np.uint64(30))) * _C1
+        z = (z ^ (z >> np.uint64(27))) * _C2
+    return z ^ (z >> np.uint64(31))
+
+
+def _state(seed: int) -> np.uint64:
+    with np.errstate(over="ignore"):
+        return _mix(np.array([np.uint64(seed) + _GAMMA], dtype=np.uint64))[0]
+
+
+def _stream(state, idx: np.ndarray) -> np.ndarray:
+    with np.errstate(over="ignore"):
+        return _mix(np.uint64(state) + (idx.astype(np.uint64) + np.uint64(1)) * _GAMMA)
+
+
+def _unit(r: np.ndarray) -> np.ndarray:
+    return (r >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def _scale_to(r: np.ndarray, n: int) -> np.ndarray:
+    """floor(r * n / 2^64) for n < 2^32."""
+    hi, lo = r >> np.uint64(32), r & np.uint64(0xFFFFFFFF)
+    n = np.uint64(n)
+    return ((hi * n + ((lo * n) >> np.uint64(32))) >> np.uint64(32)).astype(np.uint32)
+
+
+def symmetric_csr(n: int, src: np.ndarray, dst: np.ndarray):
+    """Symmetric, loop-free, deduplicated CSR of undirected pairs."""
+    keep = src != dst
+    s = np.concatenate([src[keep], dst[keep]]).astype(np.uint64)
+    d = np.concatenate([dst[keep], src[keep]]).astype(np.uint64)
+    keys = np.unique((s << np.uint64(32)) | d)
+    offsets = np.zeros(n + 1, dtype=np.uint32)
+    np.add.at(offsets, (keys >> np.uint64(32)).astype(np.int64) + 1, 1)
+    return np.cumsum(offsets, dtype=np.uint64).astype(np.uint32), (keys & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+
+
+def grid_pairs(width: int, height: int, drop: float, seed: int):
+    horizontal = height * (width - 1)
+    e = np.arange(horizontal + (height - 1) * width, dtype=np.uint64)
+    keep = _unit(_stream(_state(seed), e)) >= drop
+    y, x = e // max(width - 1, 1), e % max(width - 1, 1)
+    src = np.where(e < horizontal, y * width + x, e - horizontal)
+    dst = np.where(e < horizontal, src + 1, src + width)
+    return src[keep].astype(np.uint32), dst[keep].astype(np.uint32)
+
+
+def watts_strogatz_pairs(n: int, k: int, p: float, seed: int):
+    half = k // 2
+    idx = np.arange(n * half, dtype=np.uint64)
+    state = _state(seed)
+    src = idx // np.uint64(half)
+    j = idx - src * np.uint64(half) + np.uint64(1)
+    dst = ((src + j) % np.uint64(n)).astype(np.uint32)
+    rewire = _unit(_stream(state, 2 * idx)) < p
+    dst = np.where(rewire, _scale_to(_stream(state, 2 * idx + np.uint64(1)), n), dst)
+    return src.astype(np.uint32), dst.astype(np.uint32)
+
+
+def geometric_pairs(n: int, avg_degree: float, seed: int):
+    """All pairs within r, (n - 1) pi r^2 = avg_degree (O(n^2): small n)."""
+    i = np.arange(n, dtype=np.uint64)
+    state = _state(seed)
+    x, y = _unit(_stream(state, 2 * i)), _unit(_stream(state, 2 * i + np.uint64(1)))
+    r = np.sqrt(avg_degree / (np.pi * (n - 1))) if n > 1 else 1.0
+    r2 = r * r
+    dx = x[:, None] - x[None, :]
+    dy = y[:, None] - y[None, :]
+    a, b = np.nonzero(np.triu((dx * dx + dy * dy) <= r2, k=1))
+    return a.astype(np.uint32), b.astype(np.uint32)
