@@ -15,15 +15,24 @@
 //    vertex scans its list for a parent in the frontier bitmap and stops at the
 //    first hit (Beamer, Asanovic and Patterson, SC'12). No atomics: each warp
 //    owns one bitmap word of 32 vertices.
-//  * Direction rule: Beamer's alpha/beta heuristic (alpha = 14, beta = 24),
-//    fed by the frontier and unexplored edge counts the steps emit. The
-//    direction only changes the schedule; BFS levels are unique, so the
-//    distances cannot change.
+//  * Three step variants: push with one warp per frontier vertex (one
+//    launch), load-balanced push (above), pull (above).
+//  * Schedule: Beamer's alpha/beta rule (alpha = 14, beta = 24) over the
+//    balanced push and the pull, fed by the frontier and unexplored edge
+//    counts the steps emit; or, when a learned schedule is installed on the
+//    device, a one-warp kernel after every step that turns the step's
+//    counters into features and picks the variant with the smallest predicted
+//    time (sched.cuh), with the alpha/beta rule as its fallback. The schedule
+//    only changes which kernels run; BFS levels are unique, so the distances
+//    cannot change.
+//  * Trace mode (bfs_trace) times every valid variant at every level from the
+//    same frontier: the training data of the learned schedule.
 //  * Vertices without out-edges are counted and labelled but never queued.
 #include <algorithm>
 
 #include "device_common.cuh"
 #include "gcu_internal.h"
+#include "sched.cuh"
 
 namespace gcu {
 
@@ -36,6 +45,15 @@ struct BfsCounters {
     uint32_t discovered;  // vertices labelled this level
     uint32_t queued;      // of those, vertices with out-edges (appended to the queue)
     unsigned long long edges;  // sum of out-degrees of the vertices labelled this level
+    int32_t choice;       // learned schedule's variant for the next step (-1: use the fixed rule)
+    uint32_t pad;
+};
+
+// Step variants (the learned schedule's three outputs for a BFS level).
+enum BfsVariant : int {
+    kPushWarp = 0,      // top-down, one warp per frontier vertex, one launch
+    kPushBalanced = 1,  // top-down, frontier edges split evenly over blocks (degrees + scan + expand)
+    kPull = 2,          // bottom-up over the frontier bitmap (symmetric graphs only)
 };
 
 struct BfsWork {
@@ -206,6 +224,53 @@ __global__ void __launch_bounds__(kBuThreads) bfs_bottomup_kernel(
     }
 }
 
+// Top-down, one warp per frontier vertex (no degree scan: one launch, for
+// frontiers whose edges are few or evenly spread).
+__global__ void __launch_bounds__(kTdThreads) bfs_topdown_warp_kernel(
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, const uint32_t* __restrict__ queue,
+    uint32_t qsize, int32_t* __restrict__ dist, uint32_t* __restrict__ visited, uint32_t* __restrict__ next_queue,
+    BfsCounters* __restrict__ ctr, int32_t next_level) {
+    const unsigned lane = lane_id();
+    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    for (uint64_t i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < qsize; i += nwarps) {
+        const uint32_t u = queue[i];
+        const uint64_t s = offsets[u], e = offsets[u + 1];
+        for (uint64_t b = s; b < e; b += 32) {
+            const uint64_t j = b + lane;
+            bool found = false;
+            uint32_t v = 0;
+            if (j < e) {
+                v = ld_stream(targets + j);
+                const uint32_t bit = 1u << (v & 31);
+                if (!(__ldcg(visited + (v >> 5)) & bit)) found = !(atomicOr(visited + (v >> 5), bit) & bit);
+            }
+            record_discovery(found, v, offsets, dist, next_level, next_queue, ctr);
+        }
+    }
+}
+
+// One warp: the features of the decision before expanding the frontier the
+// last step produced (its counters, plus the host's totals before that step),
+// written to features_out when given; with a network, the chosen variant goes
+// to ctr->choice for the host to read with the counters.
+__global__ void bfs_decide_kernel(const __nv_bfloat16* __restrict__ w, BfsCounters* __restrict__ ctr,
+                                  DegreeStats stats, unsigned long long prior_unexplored, uint32_t prior_reached,
+                                  int32_t frontier_level, int frontier_bitmap, unsigned valid_mask,
+                                  float* __restrict__ features_out) {
+    const BfsCounters c = *ctr;
+    float f[kSchedIn];
+    bfs_features(f, static_cast<float>(c.discovered), static_cast<float>(c.edges),
+                 static_cast<float>(prior_unexplored - c.edges), frontier_level, stats, frontier_bitmap != 0,
+                 static_cast<float>(prior_reached + c.discovered));
+    if (features_out && lane_id() == 0)
+        for (int k = 0; k < kSchedIn; ++k) features_out[k] = f[k];
+    if (w) {
+        float out[kSchedOut];
+        sched_forward_warp(w, f, out);
+        if (lane_id() == 0) ctr->choice = sched_pick(out, valid_mask);
+    }
+}
+
 // ---------------------------------------------------------------- host
 
 static Error ensure_work(GraphImpl& g) {
@@ -231,90 +296,262 @@ static Error ensure_work(GraphImpl& g) {
     return ok();
 }
 
+namespace {
+
+// Where a level-synchronous run stands between two steps.
+struct BfsState {
+    uint32_t frontier_n = 0;    // vertices labelled by the last step
+    uint32_t frontier_q = 0;    // of those, queued (out-degree > 0)
+    uint64_t frontier_m = 0;    // their out-edges
+    uint64_t unexplored = 0;    // out-edges of vertices not labelled yet
+    uint32_t reached = 0;
+    int32_t level = 0;          // level of the frontier
+    int cur = 0;                // queue[cur] / bitmap[cur] hold the frontier
+    bool bottom_up = false;     // the last step was a pull
+    bool bitmap_valid = false;  // bitmap[cur] holds the frontier
+};
+
+// Beamer's direction rule (alpha = 14, beta = 24) over the balanced push and
+// the pull: the fixed schedule, and the fallback of the learned one.
+int fixed_rule(const BfsState& st, bool symmetric, uint32_t V) {
+    constexpr double alpha = 14.0, beta = 24.0;
+    if (!symmetric) return kPushBalanced;
+    if (!st.bottom_up && static_cast<double>(st.frontier_m) > static_cast<double>(st.unexplored) / alpha) return kPull;
+    if (st.bottom_up && static_cast<double>(st.frontier_n) < static_cast<double>(V) / beta) return kPushBalanced;
+    return st.bottom_up ? kPull : kPushBalanced;
+}
+
+unsigned valid_variants(bool symmetric) {
+    return (1u << kPushWarp) | (1u << kPushBalanced) | (symmetric ? (1u << kPull) : 0u);
+}
+
+// Launches one step of `variant` from the frontier in st (counters reset).
+Error launch_step(GraphImpl& g, BfsWork& w, int variant, const BfsState& st) {
+    DeviceImpl& dev = *g.dev;
+    const uint32_t V = g.num_nodes;
+    const uint64_t words = ceil_div_u64(V, 32);
+    const unsigned grid_cap = static_cast<unsigned>(dev.sm_count) * 16;
+    const int cur = st.cur, nxt = cur ^ 1;
+    GCU_CUDA(cudaMemsetAsync(w.counters.ptr, 0, sizeof(BfsCounters), dev.stream), "memset");
+    if (variant == kPull) {
+        if (!st.bitmap_valid) {
+            GCU_CUDA(cudaMemsetAsync(w.bitmap[cur].ptr, 0, sizeof(uint32_t) * words, dev.stream), "memset");
+            unsigned blocks = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(st.frontier_q, 256), grid_cap));
+            GCU_LAUNCH(dev, "bfs_queue_to_bitmap", bfs_queue_to_bitmap_kernel, blocks, 256, 0, w.queue[cur].ptr,
+                       st.frontier_q, w.bitmap[cur].ptr);
+        }
+        unsigned blocks = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(words * 32, kBuThreads), grid_cap));
+        GCU_LAUNCH(dev, "bfs_bottomup", bfs_bottomup_kernel, blocks, kBuThreads, 0, g.offsets.ptr, g.targets.ptr, V,
+                   w.bitmap[cur].ptr, w.bitmap[nxt].ptr, w.visited.ptr, w.dist.ptr, w.queue[nxt].ptr, w.counters.ptr,
+                   st.level + 1);
+    } else if (variant == kPushWarp) {
+        unsigned blocks = static_cast<unsigned>(
+            std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(st.frontier_q, kTdThreads / 32), grid_cap)));
+        GCU_LAUNCH(dev, "bfs_topdown_warp", bfs_topdown_warp_kernel, blocks, kTdThreads, 0, g.offsets.ptr,
+                   g.targets.ptr, w.queue[cur].ptr, st.frontier_q, w.dist.ptr, w.visited.ptr, w.queue[nxt].ptr,
+                   w.counters.ptr, st.level + 1);
+    } else {
+        unsigned blocks = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(st.frontier_q, 256), grid_cap));
+        GCU_LAUNCH(dev, "bfs_queue_degrees", bfs_queue_degrees_kernel, blocks, 256, 0, g.offsets.ptr,
+                   w.queue[cur].ptr, st.frontier_q, w.degree_scan.ptr);
+        GCU_TRY(exclusive_scan_u32(dev, w.degree_scan.ptr, w.degree_scan.ptr, st.frontier_q));
+        unsigned td_blocks = static_cast<unsigned>(std::max<uint64_t>(1, ceil_div_u64(st.frontier_m, kTdTile)));
+        GCU_LAUNCH(dev, "bfs_topdown", bfs_topdown_kernel, td_blocks, kTdThreads, 0, g.offsets.ptr, g.targets.ptr,
+                   w.queue[cur].ptr, st.frontier_q, w.degree_scan.ptr, w.dist.ptr, w.visited.ptr, w.queue[nxt].ptr,
+                   w.counters.ptr, st.level + 1);
+    }
+    return ok();
+}
+
+// Resets the work buffers and labels the source; st describes level 0.
+Error start_run(GraphImpl& g, BfsWork& w, uint32_t source) {
+    DeviceImpl& dev = *g.dev;
+    const uint64_t words = ceil_div_u64(g.num_nodes, 32);
+    GCU_CUDA(cudaMemsetAsync(w.dist.ptr, 0xFF, sizeof(int32_t) * g.num_nodes, dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(w.visited.ptr, 0, sizeof(uint32_t) * words, dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(w.counters.ptr, 0, sizeof(BfsCounters), dev.stream), "memset");
+    GCU_LAUNCH(dev, "bfs_init", bfs_init_kernel, 1, 32, 0, g.offsets.ptr, source, w.dist.ptr, w.visited.ptr,
+               w.queue[0].ptr, w.counters.ptr);
+    return ok();
+}
+
+Error read_counters(DeviceImpl& dev, BfsWork& w) {
+    GCU_CUDA(cudaMemcpyAsync(w.host_counters, w.counters.ptr, sizeof(BfsCounters), cudaMemcpyDeviceToHost, dev.stream),
+             "copy");
+    return dev.sync();
+}
+
+// Folds the counters of the step just run (or of the init) into st.
+void advance(BfsState& st, const BfsCounters& c, bool first, int variant, uint64_t num_edges) {
+    if (first) {
+        st.unexplored = num_edges - c.edges;
+        st.reached = 1;
+        st.level = 0;
+    } else {
+        st.level += 1;
+        st.reached += c.discovered;
+        st.unexplored -= c.edges;
+        st.cur ^= 1;
+        st.bottom_up = variant == kPull;
+        st.bitmap_valid = variant == kPull;
+    }
+    st.frontier_n = c.discovered;
+    st.frontier_q = c.queued;
+    st.frontier_m = c.edges;
+}
+
+uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+}  // namespace
+
 Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reachable, int32_t* max_depth) {
     DeviceImpl& dev = *g.dev;
     GCU_TRY(ensure_work(g));
     BfsWork& w = *g.bfs_work;
-    const uint32_t V = g.num_nodes;
-    const uint64_t words = ceil_div_u64(V, 32);
-    const unsigned grid_cap = static_cast<unsigned>(dev.sm_count) * 16;
+    const bool sym = w.symmetric == 1;
+    const unsigned valid = valid_variants(sym);
+    const __nv_bfloat16* net = reinterpret_cast<const __nv_bfloat16*>(dev.schedule);
+    DegreeStats stats;
+    if (net) GCU_TRY(degree_stats(g, &stats));
 
-    GCU_CUDA(cudaMemsetAsync(w.dist.ptr, 0xFF, sizeof(int32_t) * V, dev.stream), "memset");
-    GCU_CUDA(cudaMemsetAsync(w.visited.ptr, 0, sizeof(uint32_t) * words, dev.stream), "memset");
-    GCU_LAUNCH(dev, "bfs_init", bfs_init_kernel, 1, 32, 0, g.offsets.ptr, source, w.dist.ptr, w.visited.ptr,
-               w.queue[0].ptr, w.counters.ptr);
-    GCU_CUDA(cudaMemcpyAsync(w.host_counters, w.counters.ptr, sizeof(BfsCounters), cudaMemcpyDeviceToHost, dev.stream),
-             "copy");
-    GCU_TRY(dev.sync());
-
-    const double alpha = 14.0, beta = 24.0;
-    uint64_t unexplored = static_cast<uint64_t>(g.num_edges) - w.host_counters->edges;
-    uint32_t frontier_n = w.host_counters->discovered;
-    uint32_t frontier_q = w.host_counters->queued;
-    uint64_t frontier_m = w.host_counters->edges;
-    uint32_t reached = 1;
-    int32_t level = 0;
-    int cur = 0;             // queue[cur] / bitmap[cur] hold the current frontier
-    bool bottom_up = false;  // direction of the previous step
-    bool bitmap_valid = false;
-
-    while (frontier_q > 0) {
-        bool use_bottom_up = bottom_up;
-        if (w.symmetric == 1) {
-            if (!bottom_up && static_cast<double>(frontier_m) > static_cast<double>(unexplored) / alpha)
-                use_bottom_up = true;
-            else if (bottom_up && static_cast<double>(frontier_n) < static_cast<double>(V) / beta)
-                use_bottom_up = false;
-        } else {
-            use_bottom_up = false;
+    GCU_TRY(start_run(g, w, source));
+    if (net)
+        GCU_LAUNCH(dev, "bfs_decide", bfs_decide_kernel, 1, 32, 0, net, w.counters.ptr, stats,
+                   static_cast<unsigned long long>(g.num_edges), 0u, 0, 0, valid, nullptr);
+    GCU_TRY(read_counters(dev, w));
+    BfsState st;
+    advance(st, *w.host_counters, true, 0, g.num_edges);
+    while (st.frontier_q > 0) {
+        int variant = fixed_rule(st, sym, g.num_nodes);
+        if (net) {
+            const int c = w.host_counters->choice;
+            if (c >= 0 && ((valid >> c) & 1u)) variant = c;
         }
-        const int nxt = cur ^ 1;
-        GCU_CUDA(cudaMemsetAsync(w.counters.ptr, 0, sizeof(BfsCounters), dev.stream), "memset");
-        if (use_bottom_up) {
-            if (!bitmap_valid) {
-                GCU_CUDA(cudaMemsetAsync(w.bitmap[cur].ptr, 0, sizeof(uint32_t) * words, dev.stream), "memset");
-                unsigned blocks = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(frontier_q, 256), grid_cap));
-                GCU_LAUNCH(dev, "bfs_queue_to_bitmap", bfs_queue_to_bitmap_kernel, blocks, 256, 0, w.queue[cur].ptr,
-                           frontier_q, w.bitmap[cur].ptr);
-            }
-            unsigned blocks = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(words * 32, kBuThreads), grid_cap));
-            GCU_LAUNCH(dev, "bfs_bottomup", bfs_bottomup_kernel, blocks, kBuThreads, 0, g.offsets.ptr, g.targets.ptr,
-                       V, w.bitmap[cur].ptr, w.bitmap[nxt].ptr, w.visited.ptr, w.dist.ptr, w.queue[nxt].ptr,
-                       w.counters.ptr, level + 1);
-            bitmap_valid = true;
-        } else {
-            unsigned blocks = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(frontier_q, 256), grid_cap));
-            GCU_LAUNCH(dev, "bfs_queue_degrees", bfs_queue_degrees_kernel, blocks, 256, 0, g.offsets.ptr,
-                       w.queue[cur].ptr, frontier_q, w.degree_scan.ptr);
-            GCU_TRY(exclusive_scan_u32(dev, w.degree_scan.ptr, w.degree_scan.ptr, frontier_q));
-            unsigned td_blocks = static_cast<unsigned>(std::max<uint64_t>(1, ceil_div_u64(frontier_m, kTdTile)));
-            GCU_LAUNCH(dev, "bfs_topdown", bfs_topdown_kernel, td_blocks, kTdThreads, 0, g.offsets.ptr, g.targets.ptr,
-                       w.queue[cur].ptr, frontier_q, w.degree_scan.ptr, w.dist.ptr, w.visited.ptr, w.queue[nxt].ptr,
-                       w.counters.ptr, level + 1);
-            bitmap_valid = false;
-        }
-        bottom_up = use_bottom_up;
-        GCU_CUDA(cudaMemcpyAsync(w.host_counters, w.counters.ptr, sizeof(BfsCounters), cudaMemcpyDeviceToHost,
-                                 dev.stream),
-                 "copy");
-        GCU_TRY(dev.sync());
-        const BfsCounters c = *w.host_counters;
-        if (c.discovered == 0) break;
-        level += 1;
-        reached += c.discovered;
-        unexplored -= c.edges;
-        frontier_n = c.discovered;
-        frontier_q = c.queued;
-        frontier_m = c.edges;
-        cur = nxt;
+        GCU_TRY(launch_step(g, w, variant, st));
+        if (net)
+            GCU_LAUNCH(dev, "bfs_decide", bfs_decide_kernel, 1, 32, 0, net, w.counters.ptr, stats,
+                       static_cast<unsigned long long>(st.unexplored), st.reached, st.level + 1,
+                       variant == kPull ? 1 : 0, valid, nullptr);
+        GCU_TRY(read_counters(dev, w));
+        if (w.host_counters->discovered == 0) break;
+        advance(st, *w.host_counters, false, variant, g.num_edges);
     }
     if (host_distances) {
-        GCU_CUDA(cudaMemcpyAsync(host_distances, w.dist.ptr, sizeof(int32_t) * V, cudaMemcpyDeviceToHost, dev.stream),
+        GCU_CUDA(cudaMemcpyAsync(host_distances, w.dist.ptr, sizeof(int32_t) * g.num_nodes, cudaMemcpyDeviceToHost,
+                                 dev.stream),
                  "copy distances to host");
         GCU_TRY(dev.sync());
     }
-    *reachable = reached;
-    *max_depth = level;
+    *reachable = st.reached;
+    *max_depth = st.level;
+    return ok();
+}
+
+// Trace: at every level, each valid variant runs from the same frontier
+// (visited bitmap and distances restored from a snapshot in between) and is
+// timed with events on the stream; all must label the same vertices. The run
+// then continues with the fixed rule's variant, or, for 3 levels in 10 chosen
+// by explore_seed, a uniformly drawn valid one (so that the traces also hold
+// states the fixed rule never reaches).
+Error bfs_trace(GraphImpl& g, uint32_t source, uint64_t explore_seed, std::vector<BfsTraceLevel>* levels) {
+    DeviceImpl& dev = *g.dev;
+    GCU_TRY(ensure_work(g));
+    BfsWork& w = *g.bfs_work;
+    const bool sym = w.symmetric == 1;
+    const unsigned valid = valid_variants(sym);
+    DegreeStats stats;
+    GCU_TRY(degree_stats(g, &stats));
+    const uint64_t V = g.num_nodes, words = ceil_div_u64(V, 32);
+    DeviceBuffer<uint32_t> visited_snap;
+    DeviceBuffer<int32_t> dist_snap;
+    DeviceBuffer<BfsCounters> variant_ctr;
+    DeviceBuffer<float> feats;
+    GCU_TRY(visited_snap.allocate(dev, words));
+    GCU_TRY(dist_snap.allocate(dev, V));
+    GCU_TRY(variant_ctr.allocate(dev, kSchedOut));
+    cudaEvent_t ev[2 * kSchedOut];
+    for (auto& e : ev) GCU_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+    struct Events {
+        cudaEvent_t* e;
+        ~Events() {
+            for (int i = 0; i < 2 * kSchedOut; ++i) cudaEventDestroy(e[i]);
+        }
+    } guard{ev};
+
+    levels->clear();
+    GCU_TRY(feats.allocate(dev, kSchedIn));
+    GCU_TRY(start_run(g, w, source));
+    GCU_LAUNCH(dev, "bfs_decide", bfs_decide_kernel, 1, 32, 0, nullptr, w.counters.ptr, stats,
+               static_cast<unsigned long long>(g.num_edges), 0u, 0, 0, valid, feats.ptr);
+    GCU_TRY(read_counters(dev, w));
+    BfsState st;
+    advance(st, *w.host_counters, true, 0, g.num_edges);
+    std::vector<float> host_feats(kSchedIn);
+    GCU_CUDA(cudaMemcpy(host_feats.data(), feats.ptr, 4 * kSchedIn, cudaMemcpyDeviceToHost), "copy");
+    while (st.frontier_q > 0) {
+        BfsTraceLevel rec{};
+        for (int k = 0; k < kSchedIn; ++k) rec.features[k] = host_feats[k];
+        rec.valid = static_cast<uint8_t>(valid);
+        const int fixed = fixed_rule(st, sym, g.num_nodes);
+        rec.fixed_rule = static_cast<uint8_t>(fixed);
+        int take = fixed;
+        const uint64_t r = mix64(explore_seed * 0x9E3779B97F4A7C15ull + static_cast<uint64_t>(st.level) + 1);
+        if (r % 10 < 3) {
+            const int nvalid = __builtin_popcount(valid);
+            int pick = static_cast<int>((r >> 32) % nvalid);
+            for (int c = 0; c < kSchedOut; ++c)
+                if ((valid >> c) & 1u) {
+                    if (pick == 0) {
+                        take = c;
+                        break;
+                    }
+                    --pick;
+                }
+        }
+        rec.taken = static_cast<uint8_t>(take);
+        GCU_CUDA(cudaMemcpyAsync(visited_snap.ptr, w.visited.ptr, 4 * words, cudaMemcpyDeviceToDevice, dev.stream),
+                 "copy");
+        GCU_CUDA(cudaMemcpyAsync(dist_snap.ptr, w.dist.ptr, 4 * V, cudaMemcpyDeviceToDevice, dev.stream), "copy");
+        for (int k = 0; k < kSchedOut; ++k) {
+            const int c = (k + st.level) % kSchedOut;  // rotate which variant goes first
+            if (!((valid >> c) & 1u)) continue;
+            GCU_CUDA(cudaEventRecord(ev[2 * c], dev.stream), "cudaEventRecord");
+            GCU_TRY(launch_step(g, w, c, st));
+            GCU_CUDA(cudaEventRecord(ev[2 * c + 1], dev.stream), "cudaEventRecord");
+            GCU_CUDA(cudaMemcpyAsync(variant_ctr.ptr + c, w.counters.ptr, sizeof(BfsCounters),
+                                     cudaMemcpyDeviceToDevice, dev.stream),
+                     "copy");
+            GCU_CUDA(cudaMemcpyAsync(w.visited.ptr, visited_snap.ptr, 4 * words, cudaMemcpyDeviceToDevice, dev.stream),
+                     "copy");
+            GCU_CUDA(cudaMemcpyAsync(w.dist.ptr, dist_snap.ptr, 4 * V, cudaMemcpyDeviceToDevice, dev.stream), "copy");
+        }
+        GCU_TRY(launch_step(g, w, take, st));
+        GCU_LAUNCH(dev, "bfs_decide", bfs_decide_kernel, 1, 32, 0, nullptr, w.counters.ptr, stats,
+                   static_cast<unsigned long long>(st.unexplored), st.reached, st.level + 1, take == kPull ? 1 : 0,
+                   valid, feats.ptr);
+        BfsCounters vc[kSchedOut];
+        GCU_CUDA(cudaMemcpyAsync(vc, variant_ctr.ptr, sizeof(vc), cudaMemcpyDeviceToHost, dev.stream), "copy");
+        GCU_CUDA(cudaMemcpyAsync(host_feats.data(), feats.ptr, 4 * kSchedIn, cudaMemcpyDeviceToHost, dev.stream),
+                 "copy");
+        GCU_TRY(read_counters(dev, w));
+        const BfsCounters c = *w.host_counters;
+        for (int v = 0; v < kSchedOut; ++v) {
+            rec.times_us[v] = __builtin_nanf("");
+            if (!((valid >> v) & 1u)) continue;
+            if (vc[v].discovered != c.discovered || vc[v].queued != c.queued || vc[v].edges != c.edges)
+                return kernel_error("BFS step variants disagree at level " + std::to_string(st.level));
+            float ms = 0.f;
+            GCU_CUDA(cudaEventElapsedTime(&ms, ev[2 * v], ev[2 * v + 1]), "cudaEventElapsedTime");
+            rec.times_us[v] = 1000.f * ms;
+        }
+        levels->push_back(rec);
+        if (c.discovered == 0) break;
+        advance(st, c, false, take, g.num_edges);
+    }
     return ok();
 }
 

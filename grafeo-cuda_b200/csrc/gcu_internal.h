@@ -102,6 +102,10 @@ struct DeviceImpl {
     std::vector<Pending> pending;
     std::vector<cudaEvent_t> event_pool;
 
+    // Installed learned-schedule network (BF16 bit patterns, device copy);
+    // NULL: the fixed rules (alpha/beta BFS direction, degree-range buckets).
+    uint16_t* schedule = nullptr;
+
     ~DeviceImpl();
 
     // Makes this device current on the calling thread.
@@ -156,6 +160,14 @@ struct DeviceBuffer {
 struct PageRankPlan;
 struct BfsWork;
 
+// Per-graph degree statistics that the learned schedule's features use.
+struct DegreeStats {
+    float mean_degree = 0.f;
+    float max_degree = 0.f;
+    float gini = 0.f;  // Gini coefficient of the degree distribution
+    float num_nodes = 0.f;
+};
+
 struct GraphImpl {
     std::shared_ptr<DeviceImpl> dev;
     uint32_t num_nodes = 0;
@@ -167,6 +179,8 @@ struct GraphImpl {
     PageRankPlan* pr_plan = nullptr;  // owned; freed by destroy_pagerank_plan
     PageRankPlan* pr_plan_directed = nullptr;  // pull over the transpose; owned
     BfsWork* bfs_work = nullptr;      // owned; freed by destroy_bfs_work
+    bool has_degree_stats = false;
+    DegreeStats degree_stats;
     ~GraphImpl();
 };
 
@@ -256,6 +270,45 @@ struct GeneratorSpec {
     double avg_degree = 0;                // geometric
 };
 Error generate_graph(DeviceImpl& dev, const GeneratorSpec& spec, GraphImpl& g);
+
+// ---------------------------------------------------------------- learned schedule
+
+// Degree statistics of the CSR lists (computed on the device once, cached;
+// the caller holds g.mu like every algorithm entry point).
+Error degree_stats(GraphImpl& g, DegreeStats* out);
+
+// Batched forward pass: out[n][3] predictions of features x[n][12].
+Error sched_forward(DeviceImpl& dev, const uint16_t* weights, const float* x, uint64_t n, float* out);
+// Masked mean squared error of the predictions against y[n][3] (mask[n][3]
+// selects the recorded variants) and its gradient w.r.t. the 1571 parameters.
+Error sched_gradient(DeviceImpl& dev, const uint16_t* weights, const float* x, const float* y, const uint8_t* mask,
+                     uint64_t n, double* loss, float* grad);
+// Adam on the device over minibatches drawn with replacement; master (FP32)
+// is updated in place and weights receives its BF16 rounding.
+Error sched_train(DeviceImpl& dev, float* master, uint16_t* weights, const float* x, const float* y,
+                  const uint8_t* mask, uint64_t n, uint32_t steps, uint32_t batch, float lr, uint64_t seed,
+                  double* final_loss);
+Error set_schedule(DeviceImpl& dev, const uint16_t* weights);
+
+// Per-level BFS trace: every valid step variant timed from the same frontier.
+struct BfsTraceLevel {
+    float features[12];
+    float times_us[3];  // NaN for a variant that is not valid here
+    uint8_t valid;      // bit c: variant c valid
+    uint8_t fixed_rule; // what the alpha/beta rule picks
+    uint8_t taken;      // the variant the traced run continued with
+};
+Error bfs_trace(GraphImpl& g, uint32_t source, uint64_t explore_seed, std::vector<BfsTraceLevel>* levels);
+
+// Per-bucket triangle trace: every valid intersection variant timed per
+// out-degree bucket of the DAG; *total = the triangle count (all agree).
+struct TcTraceBucket {
+    float features[12];
+    float times_us[3];
+    uint8_t valid;
+    uint8_t fixed_rule;
+};
+Error triangle_trace(GraphImpl& g, std::vector<TcTraceBucket>* buckets, uint64_t* total);
 
 }  // namespace gcu
 

@@ -9,6 +9,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <sstream>
 
 #include "gcu_internal.h"
@@ -57,6 +58,7 @@ gcu_status succeed() {
 
 DeviceImpl::~DeviceImpl() {
     cudaSetDevice(ordinal);
+    if (schedule && stream) cudaFreeAsync(schedule, stream);
     if (stream) cudaStreamSynchronize(stream);
     collect_pending();
     for (auto e : event_pool) cudaEventDestroy(e);
@@ -649,6 +651,91 @@ GCU_API gcu_status gcu_truss_decomposition(gcu_graph* g, uint32_t* trussness, ui
     if (max_trussness) *max_trussness = top;
     if (rounds) *rounds = r;
     if (seconds) *seconds = wall.seconds();
+    return succeed();
+}
+
+static gcu_status on_device(gcu_device* dev, const std::function<Error(DeviceImpl&)>& body) {
+    if (!dev) return fail(kernel_error("device is NULL"));
+    DeviceImpl& d = *dev->impl;
+    Error e = d.activate();
+    if (e.ok()) e = body(d);
+    return e.ok() ? succeed() : fail(e);
+}
+
+GCU_API gcu_status gcu_device_set_schedule(gcu_device* dev, const uint16_t* weights) {
+    return on_device(dev, [&](DeviceImpl& d) { return set_schedule(d, weights); });
+}
+
+GCU_API gcu_status gcu_schedule_forward(gcu_device* dev, const uint16_t* weights, const float* features, size_t n,
+                                        float* out) {
+    if (!weights || (n && (!features || !out))) return fail(kernel_error("gcu_schedule_forward: NULL argument"));
+    return on_device(dev, [&](DeviceImpl& d) { return sched_forward(d, weights, features, n, out); });
+}
+
+GCU_API gcu_status gcu_schedule_gradient(gcu_device* dev, const uint16_t* weights, const float* features,
+                                         const float* targets, const uint8_t* mask, size_t n, double* loss,
+                                         float* grad) {
+    if (!weights || !loss || !grad || (n && (!features || !targets || !mask)))
+        return fail(kernel_error("gcu_schedule_gradient: NULL argument"));
+    return on_device(dev, [&](DeviceImpl& d) { return sched_gradient(d, weights, features, targets, mask, n, loss, grad); });
+}
+
+GCU_API gcu_status gcu_schedule_train(gcu_device* dev, float* master, uint16_t* weights, const float* features,
+                                      const float* targets, const uint8_t* mask, size_t n, uint32_t steps,
+                                      uint32_t batch, float lr, uint64_t seed, double* final_loss) {
+    if (!master || !weights || !final_loss || (n && (!features || !targets || !mask)))
+        return fail(kernel_error("gcu_schedule_train: NULL argument"));
+    return on_device(dev, [&](DeviceImpl& d) {
+        return sched_train(d, master, weights, features, targets, mask, n, steps, batch, lr, seed, final_loss);
+    });
+}
+
+GCU_API gcu_status gcu_bfs_trace(gcu_graph* g, uint32_t source, uint64_t explore_seed, float* features,
+                                 float* times_us, uint8_t* valid, uint8_t* fixed_rule, uint8_t* taken,
+                                 size_t capacity, size_t* levels) {
+    if (!g || !levels) return fail(kernel_error("gcu_bfs_trace: NULL argument"));
+    if (capacity && (!features || !times_us || !valid || !fixed_rule || !taken))
+        return fail(kernel_error("gcu_bfs_trace: NULL output array"));
+    GraphImpl& gi = *g->impl;
+    if (source >= gi.num_nodes)
+        return fail(kernel_error("source node " + std::to_string(source) + " out of range (num_nodes = " +
+                                 std::to_string(gi.num_nodes) + ")"));
+    std::lock_guard<std::mutex> lock(gi.mu);
+    Error e = gi.dev->activate();
+    std::vector<BfsTraceLevel> rec;
+    if (e.ok()) e = bfs_trace(gi, source, explore_seed, &rec);
+    if (!e.ok()) return fail(e);
+    for (size_t i = 0; i < std::min(capacity, rec.size()); ++i) {
+        std::memcpy(features + 12 * i, rec[i].features, sizeof(rec[i].features));
+        std::memcpy(times_us + 3 * i, rec[i].times_us, sizeof(rec[i].times_us));
+        valid[i] = rec[i].valid;
+        fixed_rule[i] = rec[i].fixed_rule;
+        taken[i] = rec[i].taken;
+    }
+    *levels = rec.size();
+    return succeed();
+}
+
+GCU_API gcu_status gcu_triangle_trace(gcu_graph* g, float* features, float* times_us, uint8_t* valid,
+                                      uint8_t* fixed_rule, size_t capacity, size_t* buckets, uint64_t* total) {
+    if (!g || !buckets || !total) return fail(kernel_error("gcu_triangle_trace: NULL argument"));
+    if (capacity && (!features || !times_us || !valid || !fixed_rule))
+        return fail(kernel_error("gcu_triangle_trace: NULL output array"));
+    GraphImpl& gi = *g->impl;
+    std::lock_guard<std::mutex> lock(gi.mu);
+    Error e = gi.dev->activate();
+    std::vector<TcTraceBucket> rec;
+    uint64_t t = 0;
+    if (e.ok()) e = triangle_trace(gi, &rec, &t);
+    if (!e.ok()) return fail(e);
+    for (size_t i = 0; i < std::min(capacity, rec.size()); ++i) {
+        std::memcpy(features + 12 * i, rec[i].features, sizeof(rec[i].features));
+        std::memcpy(times_us + 3 * i, rec[i].times_us, sizeof(rec[i].times_us));
+        valid[i] = rec[i].valid;
+        fixed_rule[i] = rec[i].fixed_rule;
+    }
+    *buckets = rec.size();
+    *total = t;
     return succeed();
 }
 

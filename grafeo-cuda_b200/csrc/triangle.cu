@@ -20,14 +20,17 @@
 //     shared memory, then walks the wedges (v, w), v in N+(u), w in N+(v), 32 at
 //     a time with the (v, w) pairs balanced over the lanes by a warp scan of
 //     the d+(v), and probes each w in a shared-memory hash table of N+(u)
-//     (wedge.cuh). Out-lists longer than 128 entries go to a CTA-per-vertex
-//     kernel with a larger table (global binary search beyond 2048 entries).
+//     (wedge.cuh). Vertices are bucketed by ceil(log2 d+); each bucket runs
+//     one of three variants (warp hash table up to 128 entries, CTA hash table
+//     up to 2048, CTA binary search beyond), by the fixed degree ranges or by
+//     an installed learned schedule (sched.cuh).
 //  All indices are 64-bit where they can exceed 2^32, so there is no cap on the
 //  number of edges.
 #include <algorithm>
 
 #include "device_common.cuh"
 #include "gcu_internal.h"
+#include "sched.cuh"
 #include "wedge.cuh"
 
 namespace gcu {
@@ -153,30 +156,249 @@ Error build_dag(GraphImpl& g, bool by_degree, const uint32_t* rev, DeviceBuffer<
     return ok();
 }
 
-static Error count_dag(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets, uint32_t V,
-                       uint32_t min_deg, uint64_t* total) {
-    DeviceBuffer<unsigned long long> d_total;
-    GCU_TRY(d_total.allocate(dev, 1));
-    GCU_CUDA(cudaMemsetAsync(d_total.ptr, 0, sizeof(unsigned long long), dev.stream), "memset");
-    GCU_TRY(run_wedges(dev, d_offsets, d_targets, V, min_deg, CountSink{d_total.ptr, 0}, "tc"));
-    unsigned long long host_total = 0;
-    GCU_CUDA(cudaMemcpyAsync(&host_total, d_total.ptr, sizeof(host_total), cudaMemcpyDeviceToHost, dev.stream),
+// ---------------------------------------------------------------- out-degree buckets
+//
+// Vertices with d+ >= min_deg are grouped by c = ceil(log2 d+) (bucket c holds
+// out-degrees in (2^(c-1), 2^c]); each bucket runs one intersection variant:
+//   0  warp per vertex, shared hash table  (valid for d+ <= 128, c <= 7)
+//   1  CTA per vertex, shared hash table   (valid for d+ <= 2048, c <= 11)
+//   2  CTA per vertex, binary search of the out-list in global memory (any d+)
+// The fixed rule takes the first valid one; an installed learned schedule
+// takes the valid variant with the smallest predicted time. Buckets run from
+// the highest out-degrees down.
+
+constexpr int kBuckets = 33;
+
+__device__ __forceinline__ int bucket_of(uint32_t d) { return d <= 1 ? 0 : 32 - __clz(d - 1); }
+__host__ __device__ __forceinline__ unsigned bucket_valid(int c) { return c <= 7 ? 7u : (c <= 11 ? 6u : 4u); }
+__host__ __device__ __forceinline__ int bucket_fixed(int c) { return c <= 7 ? 0 : (c <= 11 ? 1 : 2); }
+
+__global__ void tc_bucket_count_kernel(const uint32_t* __restrict__ offsets, uint32_t V, uint32_t min_deg,
+                                       uint32_t* __restrict__ counts, unsigned long long* __restrict__ entries) {
+    __shared__ uint32_t s_count[kBuckets];
+    __shared__ unsigned long long s_entries[kBuckets];
+    if (threadIdx.x < kBuckets) {
+        s_count[threadIdx.x] = 0;
+        s_entries[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    for (uint64_t u = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u < V;
+         u += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t d = offsets[u + 1] - offsets[u];
+        if (d < min_deg || d == 0) continue;
+        const int c = bucket_of(d);
+        atomicAdd(&s_count[c], 1u);
+        atomicAdd(&s_entries[c], static_cast<unsigned long long>(d));
+    }
+    __syncthreads();
+    if (threadIdx.x < kBuckets && s_count[threadIdx.x]) {
+        atomicAdd(counts + threadIdx.x, s_count[threadIdx.x]);
+        atomicAdd(entries + threadIdx.x, s_entries[threadIdx.x]);
+    }
+}
+
+// cursor[c] starts at bucket c's first list slot.
+__global__ void tc_bucket_fill_kernel(const uint32_t* __restrict__ offsets, uint32_t V, uint32_t min_deg,
+                                      uint32_t* __restrict__ cursor, uint32_t* __restrict__ list) {
+    for (uint64_t u = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u < V;
+         u += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t d = offsets[u + 1] - offsets[u];
+        if (d < min_deg || d == 0) continue;
+        list[atomicAdd(cursor + bucket_of(d), 1u)] = static_cast<uint32_t>(u);
+    }
+}
+
+// One warp: features of every non-empty bucket (to features[c][12] when
+// given) and, with a network, the chosen variant per bucket (-1: fixed rule).
+__global__ void tc_decide_kernel(const __nv_bfloat16* __restrict__ w, const uint32_t* __restrict__ counts,
+                                 const unsigned long long* __restrict__ entries, DegreeStats stats, float dag_edges,
+                                 int* __restrict__ choices, float* __restrict__ features) {
+    for (int c = 0; c < kBuckets; ++c) {
+        if (lane_id() == 0) choices[c] = -1;
+        if (counts[c] == 0) continue;
+        const float hi = static_cast<float>(1ull << c), lo = c == 0 ? 1.f : static_cast<float>((1ull << (c - 1)) + 1);
+        float f[kSchedIn];
+        bucket_features(f, static_cast<float>(counts[c]), static_cast<float>(entries[c]), dag_edges, stats, lo, hi,
+                        stats.num_nodes > 0.f ? dag_edges / stats.num_nodes : 0.f);
+        if (features && lane_id() == 0)
+            for (int k = 0; k < kSchedIn; ++k) features[c * kSchedIn + k] = f[k];
+        if (w) {
+            float out[kSchedOut];
+            sched_forward_warp(w, f, out);
+            if (lane_id() == 0) choices[c] = sched_pick(out, bucket_valid(c));
+        }
+    }
+}
+
+namespace {
+
+struct BucketPlan {
+    DeviceBuffer<uint32_t> list, counts, cursor;
+    DeviceBuffer<unsigned long long> entries;
+    DeviceBuffer<int> choices;
+    DeviceBuffer<float> features;
+    uint32_t host_counts[kBuckets] = {};
+    uint32_t host_starts[kBuckets] = {};
+    int host_choices[kBuckets] = {};
+    float host_features[kBuckets * kSchedIn] = {};
+};
+
+// Buckets the vertices of a DAG and runs the decide kernel.
+Error plan_buckets(DeviceImpl& dev, const uint32_t* d_offsets, uint32_t V, uint32_t min_deg, uint32_t m,
+                   const DegreeStats& stats, bool want_features, BucketPlan& p) {
+    GCU_TRY(p.counts.allocate(dev, kBuckets));
+    GCU_TRY(p.cursor.allocate(dev, kBuckets));
+    GCU_TRY(p.entries.allocate(dev, kBuckets));
+    GCU_TRY(p.choices.allocate(dev, kBuckets));
+    GCU_TRY(p.features.allocate(dev, kBuckets * kSchedIn));
+    GCU_CUDA(cudaMemsetAsync(p.counts.ptr, 0, sizeof(uint32_t) * kBuckets, dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(p.entries.ptr, 0, sizeof(unsigned long long) * kBuckets, dev.stream), "memset");
+    const unsigned grid =
+        static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(V, 256), dev.sm_count * 4ull)));
+    GCU_LAUNCH(dev, "tc_bucket_count", tc_bucket_count_kernel, grid, 256, 0, d_offsets, V, min_deg, p.counts.ptr,
+               p.entries.ptr);
+    const __nv_bfloat16* net = reinterpret_cast<const __nv_bfloat16*>(dev.schedule);
+    if (net || want_features) {
+        GCU_LAUNCH(dev, "tc_decide", tc_decide_kernel, 1, 32, 0, net, p.counts.ptr, p.entries.ptr, stats,
+                   static_cast<float>(m), p.choices.ptr, want_features ? p.features.ptr : nullptr);
+        GCU_CUDA(cudaMemcpyAsync(p.host_choices, p.choices.ptr, sizeof(p.host_choices), cudaMemcpyDeviceToHost,
+                                 dev.stream),
+                 "copy");
+    } else {
+        std::fill(p.host_choices, p.host_choices + kBuckets, -1);
+    }
+    GCU_CUDA(cudaMemcpyAsync(p.host_counts, p.counts.ptr, sizeof(p.host_counts), cudaMemcpyDeviceToHost, dev.stream),
              "copy");
+    if (want_features)
+        GCU_CUDA(cudaMemcpyAsync(p.host_features, p.features.ptr, sizeof(p.host_features), cudaMemcpyDeviceToHost,
+                                 dev.stream),
+                 "copy");
     GCU_TRY(dev.sync());
-    *total = host_total;
+    uint64_t total = 0;
+    for (int c = 0; c < kBuckets; ++c) {
+        p.host_starts[c] = static_cast<uint32_t>(total);
+        total += p.host_counts[c];
+    }
+    GCU_TRY(p.list.allocate(dev, std::max<uint64_t>(total, 1)));
+    GCU_CUDA(cudaMemcpyAsync(p.cursor.ptr, p.host_starts, sizeof(p.host_starts), cudaMemcpyHostToDevice, dev.stream),
+             "copy");
+    GCU_LAUNCH(dev, "tc_bucket_fill", tc_bucket_fill_kernel, grid, 256, 0, d_offsets, V, min_deg, p.cursor.ptr,
+               p.list.ptr);
     return ok();
 }
 
-Error triangle_count(GraphImpl& g, bool oriented, uint64_t* total) {
-    *total = 0;
-    // triangle_counting.rs:44-49: nothing to count.
-    if (g.num_edges == 0) return ok();
+// One launch of `variant` over bucket c's vertices; next = its handout counter (zeroed).
+template <class Sink>
+Error launch_bucket(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets, const BucketPlan& p, int c,
+                    int variant, uint32_t* next, Sink sink) {
+    const uint32_t n = p.host_counts[c];
+    const uint32_t* list = p.list.ptr + p.host_starts[c];
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 8;
+    if (variant == 0) {
+        const unsigned grid = static_cast<unsigned>(
+            std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(n, kWedgeWarps * kVertexBatch), cap)));
+        GCU_LAUNCH(dev, "wedge_warp_bucket", wedge_warp_list_kernel<Sink>, grid, kWedgeThreads, 0, d_offsets,
+                   d_targets, list, n, next, sink);
+    } else {
+        const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(n, cap)));
+        GCU_LAUNCH(dev, variant == 1 ? "wedge_cta_bucket" : "wedge_search_bucket", wedge_cta_list_kernel<Sink>, grid,
+                   kWedgeThreads, 0, d_offsets, d_targets, list, n, next, variant == 2 ? 1 : 0, sink);
+    }
+    return ok();
+}
+
+// Sum over DAG edges u -> v of |N+(u) ∩ N+(v)| for vertices with at least
+// min_deg out-edges. With `trace`, every valid variant of every bucket runs
+// (each into its own counter), is timed, and all must agree.
+Error count_dag(GraphImpl& g, const uint32_t* d_offsets, const uint32_t* d_targets, uint32_t m, uint32_t min_deg,
+                uint64_t* total, std::vector<TcTraceBucket>* trace) {
     DeviceImpl& dev = *g.dev;
     const uint32_t V = g.num_nodes;
+    DegreeStats stats;
+    if (dev.schedule || trace) GCU_TRY(degree_stats(g, &stats));
+    BucketPlan p;
+    GCU_TRY(plan_buckets(dev, d_offsets, V, min_deg, m, stats, trace != nullptr, p));
+    const int runs = trace ? kSchedOut : 1;
+    DeviceBuffer<unsigned long long> totals;  // [bucket][variant] with trace, else [0]
+    DeviceBuffer<uint32_t> next;              // handout counters, same shape
+    GCU_TRY(totals.allocate(dev, kBuckets * runs));
+    GCU_TRY(next.allocate(dev, kBuckets * runs));
+    GCU_CUDA(cudaMemsetAsync(totals.ptr, 0, sizeof(unsigned long long) * kBuckets * runs, dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(next.ptr, 0, sizeof(uint32_t) * kBuckets * runs, dev.stream), "memset");
+    std::vector<cudaEvent_t> ev;
+    struct Events {
+        std::vector<cudaEvent_t>& e;
+        ~Events() {
+            for (auto x : e) cudaEventDestroy(x);
+        }
+    } guard{ev};
+    if (trace) {
+        ev.resize(2 * kBuckets * kSchedOut);
+        for (auto& e : ev) GCU_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+    }
+    for (int c = kBuckets - 1; c >= 0; --c) {
+        if (p.host_counts[c] == 0) continue;
+        const unsigned valid = bucket_valid(c);
+        if (!trace) {
+            int variant = bucket_fixed(c);
+            const int pick = p.host_choices[c];
+            if (pick >= 0 && ((valid >> pick) & 1u)) variant = pick;
+            GCU_TRY(launch_bucket(dev, d_offsets, d_targets, p, c, variant, next.ptr + c, CountSink{totals.ptr, 0}));
+            continue;
+        }
+        for (int v = 0; v < kSchedOut; ++v) {
+            if (!((valid >> v) & 1u)) continue;
+            const int slot = c * kSchedOut + v;
+            GCU_CUDA(cudaEventRecord(ev[2 * slot], dev.stream), "cudaEventRecord");
+            GCU_TRY(launch_bucket(dev, d_offsets, d_targets, p, c, v, next.ptr + slot,
+                                  CountSink{totals.ptr + slot, 0}));
+            GCU_CUDA(cudaEventRecord(ev[2 * slot + 1], dev.stream), "cudaEventRecord");
+        }
+    }
+    std::vector<unsigned long long> host(kBuckets * runs);
+    GCU_CUDA(cudaMemcpyAsync(host.data(), totals.ptr, sizeof(unsigned long long) * host.size(), cudaMemcpyDeviceToHost,
+                             dev.stream),
+             "copy");
+    GCU_TRY(dev.sync());
+    if (!trace) {
+        *total = host[0];
+        return ok();
+    }
+    uint64_t sum = 0;
+    trace->clear();
+    for (int c = kBuckets - 1; c >= 0; --c) {
+        if (p.host_counts[c] == 0) continue;
+        TcTraceBucket rec{};
+        std::copy(p.host_features + c * kSchedIn, p.host_features + (c + 1) * kSchedIn, rec.features);
+        rec.valid = static_cast<uint8_t>(bucket_valid(c));
+        rec.fixed_rule = static_cast<uint8_t>(bucket_fixed(c));
+        const unsigned long long expect = host[c * kSchedOut + bucket_fixed(c)];
+        for (int v = 0; v < kSchedOut; ++v) {
+            rec.times_us[v] = __builtin_nanf("");
+            if (!((rec.valid >> v) & 1u)) continue;
+            const int slot = c * kSchedOut + v;
+            if (host[slot] != expect)
+                return kernel_error("intersection variants disagree on out-degree bucket " + std::to_string(c));
+            float ms = 0.f;
+            GCU_CUDA(cudaEventElapsedTime(&ms, ev[2 * slot], ev[2 * slot + 1]), "cudaEventElapsedTime");
+            rec.times_us[v] = 1000.f * ms;
+        }
+        sum += expect;
+        trace->push_back(rec);
+    }
+    *total = sum;
+    return ok();
+}
+
+Error triangle_count_ex(GraphImpl& g, bool oriented, uint64_t* total, std::vector<TcTraceBucket>* trace) {
+    *total = 0;
+    if (trace) trace->clear();
+    // triangle_counting.rs:44-49: nothing to count.
+    if (g.num_edges == 0) return ok();
     if (oriented) {
         // The input is already a DAG: count over its lists as given; a
         // self-loop entry u -> u contributes |N(u)| like in the reference.
-        return count_dag(dev, g.offsets.ptr, g.targets.ptr, V, 1, total);
+        return count_dag(g, g.offsets.ptr, g.targets.ptr, g.num_edges, 1, total, trace);
     }
     bool symmetric = false;
     GCU_TRY(graph_symmetry(g, &symmetric));
@@ -185,7 +407,17 @@ Error triangle_count(GraphImpl& g, bool oriented, uint64_t* total) {
     GCU_TRY(build_dag(g, symmetric, nullptr, &dag_offsets, &dag_targets, nullptr, &m));
     if (m == 0) return ok();
     // A DAG vertex needs two out-neighbours to close a triangle.
-    return count_dag(dev, dag_offsets.ptr, dag_targets.ptr, V, 2, total);
+    return count_dag(g, dag_offsets.ptr, dag_targets.ptr, m, 2, total, trace);
+}
+
+}  // namespace
+
+Error triangle_count(GraphImpl& g, bool oriented, uint64_t* total) {
+    return triangle_count_ex(g, oriented, total, nullptr);
+}
+
+Error triangle_trace(GraphImpl& g, std::vector<TcTraceBucket>* buckets, uint64_t* total) {
+    return triangle_count_ex(g, false, total, buckets);
 }
 
 }  // namespace gcu

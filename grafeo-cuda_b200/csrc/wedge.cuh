@@ -226,6 +226,103 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_kernel(const uint32_t
     sink.finish();
 }
 
+// ---------------------------------------------------------------- bucket kernels
+// The same intersections over an explicit vertex list (one out-degree bucket
+// of a DAG), so that a schedule can pick the variant per bucket.
+
+// Warp per listed vertex; a shared hash table per warp for out-lists of at
+// most kWarpMaxDeg entries, binary search in global memory beyond (the
+// schedule only sends buckets within the limit here; the guard keeps the
+// table in bounds whatever the list holds).
+template <class Sink>
+__global__ void __launch_bounds__(kWedgeThreads) wedge_warp_list_kernel(const uint32_t* __restrict__ offsets,
+                                                                        const uint32_t* __restrict__ targets,
+                                                                        const uint32_t* __restrict__ list, uint32_t n,
+                                                                        uint32_t* __restrict__ next, Sink sink) {
+    constexpr bool kPos = Sink::kNeedsPos;
+    __shared__ uint32_t s_keys[kWedgeWarps][kWarpSlots];
+    __shared__ uint32_t s_pos[kPos ? kWedgeWarps : 1][kPos ? kWarpSlots : 1];
+    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_start[kWedgeWarps][32];
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    uint32_t* keys = s_keys[warp];
+    uint32_t* pos = kPos ? s_pos[warp] : nullptr;
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(next, kVertexBatch);
+        base = __shfl_sync(kFullMask, base, 0);
+        if (base >= n) break;
+        const uint32_t last = min(base + kVertexBatch, n);
+        for (uint32_t h = base; h < last; ++h) {
+            const uint32_t u = list[h];
+            const uint32_t s = offsets[u], du = offsets[u + 1] - s;
+            const bool use_table = du <= kWarpMaxDeg;
+            const uint32_t bits = use_table ? table_bits(du) : 0;
+            __syncwarp();
+            if (use_table) {
+                for (uint32_t k = lane; k < (1u << bits); k += 32) keys[k] = kEmptyKey;
+                __syncwarp();
+                for (uint32_t k = lane; k < du; k += 32) hash_insert<kPos>(keys, pos, bits, targets[s + k], k);
+                __syncwarp();
+            }
+            const uint32_t* ulist = targets + s;
+            for (uint32_t c = 0; c < du; c += 32)
+                wedge_chunk(
+                    offsets, targets, ulist, du, c, s_excl[warp], s_start[warp],
+                    [&](uint32_t w) {
+                        return use_table ? hash_find<kPos>(keys, pos, bits, w) : sorted_find(ulist, du, w);
+                    },
+                    [&](uint32_t pv, uint32_t pw, uint32_t evw) { sink.hit(s, pv, pw, evw); });
+        }
+    }
+    sink.finish();
+}
+
+// CTA per listed vertex: a shared hash table (out-lists of at most
+// kCtaMaxDeg entries, unless `search`) or binary search of the out-list in
+// global memory.
+template <class Sink>
+__global__ void __launch_bounds__(kWedgeThreads) wedge_cta_list_kernel(const uint32_t* __restrict__ offsets,
+                                                                       const uint32_t* __restrict__ targets,
+                                                                       const uint32_t* __restrict__ list, uint32_t n,
+                                                                       uint32_t* __restrict__ next, int search,
+                                                                       Sink sink) {
+    constexpr bool kPos = Sink::kNeedsPos;
+    __shared__ uint32_t s_keys[kCtaSlots];
+    __shared__ uint32_t s_pos[kPos ? kCtaSlots : 1];
+    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_start[kWedgeWarps][32];
+    __shared__ uint32_t s_item;
+    const unsigned warp = threadIdx.x >> 5;
+    uint32_t* pos = kPos ? s_pos : nullptr;
+    while (true) {
+        if (threadIdx.x == 0) s_item = atomicAdd(next, 1u);
+        __syncthreads();
+        const uint32_t h = s_item;
+        if (h >= n) break;
+        const uint32_t u = list[h];
+        const uint32_t s = offsets[u], du = offsets[u + 1] - s;
+        const uint32_t* ulist = targets + s;
+        const bool use_table = !search && du <= kCtaMaxDeg;
+        const uint32_t bits = use_table ? table_bits(du) : 0;
+        if (use_table) {
+            for (uint32_t k = threadIdx.x; k < (1u << bits); k += kWedgeThreads) s_keys[k] = kEmptyKey;
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < du; k += kWedgeThreads) hash_insert<kPos>(s_keys, pos, bits, ulist[k], k);
+            __syncthreads();
+        }
+        for (uint32_t c = warp * 32; c < du; c += kWedgeThreads)
+            wedge_chunk(
+                offsets, targets, ulist, du, c, s_excl[warp], s_start[warp],
+                [&](uint32_t w) {
+                    return use_table ? hash_find<kPos>(s_keys, pos, bits, w) : sorted_find(ulist, du, w);
+                },
+                [&](uint32_t pv, uint32_t pw, uint32_t evw) { sink.hit(s, pv, pw, evw); });
+        __syncthreads();  // the table and s_item are reused by the next list
+    }
+    sink.finish();
+}
+
 // Runs both wedge kernels over a DAG CSR: long out-lists by CTAs first (they
 // hold the heaviest work), then everything else by warps.
 template <class Sink>

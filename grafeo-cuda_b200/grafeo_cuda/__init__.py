@@ -55,6 +55,11 @@ __all__ = [
 ]
 
 
+SCHEDULE_FEATURES = 12
+SCHEDULE_OUTPUTS = 3
+SCHEDULE_PARAMS = 1571
+
+
 def version() -> str:
     return lib.gcu_version().decode()
 
@@ -145,6 +150,18 @@ class GpuDevice:
 
     def reset_stats(self) -> None:
         lib.gcu_device_reset_stats(self._h)
+
+    # -- learned schedule (grafeo_cuda.schedule trains and loads it)
+    def set_schedule(self, weights) -> None:
+        """Installs a schedule network (GCU_SCHEDULE_PARAMS BF16 bit patterns as
+        uint16) for bfs and triangle_count; None restores the fixed rules."""
+        if weights is None:
+            check(lib.gcu_device_set_schedule(self._h, None))
+            return
+        w = np.ascontiguousarray(np.asarray(weights, dtype=np.uint16))
+        if w.size != SCHEDULE_PARAMS:
+            raise ValueError(f"a schedule network has {SCHEDULE_PARAMS} parameters, got {w.size}")
+        check(lib.gcu_device_set_schedule(self._h, _ptr(w, C.c_uint16)))
 
 
 # ---------------------------------------------------------------- host CSR
@@ -484,3 +501,79 @@ class GpuGraph:
         finally:
             lib.gcu_edge_list_free(h)
         return {"edges": edges, "k": k, "iterations": int(it.value), "time_seconds": float(secs.value)}
+
+    def bfs_trace(self, source: int, explore_seed: int = 0, capacity: int = 65536) -> dict:
+        """Per-level trace of every BFS step variant (gcu_bfs_trace): features
+        [levels, 12], times_us [levels, 3] (NaN where a variant is not valid),
+        valid masks, the alpha/beta rule's picks and the variants taken."""
+        source = self._check_u32(source, "source")
+        cap = int(max(1, capacity))
+        f = np.zeros((cap, SCHEDULE_FEATURES), dtype=np.float32)
+        t = np.zeros((cap, SCHEDULE_OUTPUTS), dtype=np.float32)
+        valid = np.zeros(cap, dtype=np.uint8)
+        fixed = np.zeros(cap, dtype=np.uint8)
+        taken = np.zeros(cap, dtype=np.uint8)
+        n = C.c_size_t()
+        check(lib.gcu_bfs_trace(self._h, source, int(explore_seed), _ptr(f, C.c_float), _ptr(t, C.c_float),
+                                _ptr(valid, C.c_uint8), _ptr(fixed, C.c_uint8), _ptr(taken, C.c_uint8), cap,
+                                C.byref(n)))
+        m = min(int(n.value), cap)
+        return {"features": f[:m], "times_us": t[:m], "valid": valid[:m], "fixed_rule": fixed[:m],
+                "taken": taken[:m], "levels": int(n.value)}
+
+    def triangle_trace(self) -> dict:
+        """Per out-degree bucket trace of every intersection variant
+        (gcu_triangle_trace), plus the triangle count they all reproduce."""
+        cap = 33
+        f = np.zeros((cap, SCHEDULE_FEATURES), dtype=np.float32)
+        t = np.zeros((cap, SCHEDULE_OUTPUTS), dtype=np.float32)
+        valid = np.zeros(cap, dtype=np.uint8)
+        fixed = np.zeros(cap, dtype=np.uint8)
+        n = C.c_size_t()
+        total = C.c_uint64()
+        check(lib.gcu_triangle_trace(self._h, _ptr(f, C.c_float), _ptr(t, C.c_float), _ptr(valid, C.c_uint8),
+                                     _ptr(fixed, C.c_uint8), cap, C.byref(n), C.byref(total)))
+        m = int(n.value)
+        return {"features": f[:m], "times_us": t[:m], "valid": valid[:m], "fixed_rule": fixed[:m],
+                "total_triangles": int(total.value)}
+
+
+# ---------------------------------------------------------------- schedule network kernels
+
+
+def schedule_forward(device: GpuDevice, weights, features) -> np.ndarray:
+    """Predictions [n, 3] of the schedule network (gcu_schedule_forward)."""
+    w = np.ascontiguousarray(np.asarray(weights, dtype=np.uint16))
+    x = np.ascontiguousarray(np.asarray(features, dtype=np.float32).reshape(-1, SCHEDULE_FEATURES))
+    out = np.zeros((x.shape[0], SCHEDULE_OUTPUTS), dtype=np.float32)
+    check(lib.gcu_schedule_forward(device._h, _ptr(w, C.c_uint16), _ptr(x, C.c_float), x.shape[0],
+                                   _ptr(out, C.c_float)))
+    return out
+
+
+def schedule_gradient(device: GpuDevice, weights, features, targets, mask) -> tuple[float, np.ndarray]:
+    """(masked MSE loss, gradient [1571]) computed on the device."""
+    w = np.ascontiguousarray(np.asarray(weights, dtype=np.uint16))
+    x = np.ascontiguousarray(np.asarray(features, dtype=np.float32).reshape(-1, SCHEDULE_FEATURES))
+    y = np.ascontiguousarray(np.asarray(targets, dtype=np.float32).reshape(-1, SCHEDULE_OUTPUTS))
+    m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8).reshape(-1, SCHEDULE_OUTPUTS))
+    loss = C.c_double()
+    grad = np.zeros(SCHEDULE_PARAMS, dtype=np.float32)
+    check(lib.gcu_schedule_gradient(device._h, _ptr(w, C.c_uint16), _ptr(x, C.c_float), _ptr(y, C.c_float),
+                                    _ptr(m, C.c_uint8), x.shape[0], C.byref(loss), _ptr(grad, C.c_float)))
+    return float(loss.value), grad
+
+
+def schedule_train(device: GpuDevice, master, features, targets, mask, steps: int, batch: int = 1024,
+                   lr: float = 3e-3, seed: int = 0) -> tuple[np.ndarray, np.ndarray, float]:
+    """Adam on the device; returns (FP32 master weights, BF16 weights as uint16, final loss)."""
+    mw = np.array(master, dtype=np.float32).copy()
+    w16 = np.zeros(SCHEDULE_PARAMS, dtype=np.uint16)
+    x = np.ascontiguousarray(np.asarray(features, dtype=np.float32).reshape(-1, SCHEDULE_FEATURES))
+    y = np.ascontiguousarray(np.asarray(targets, dtype=np.float32).reshape(-1, SCHEDULE_OUTPUTS))
+    m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8).reshape(-1, SCHEDULE_OUTPUTS))
+    loss = C.c_double()
+    check(lib.gcu_schedule_train(device._h, _ptr(mw, C.c_float), _ptr(w16, C.c_uint16), _ptr(x, C.c_float),
+                                 _ptr(y, C.c_float), _ptr(m, C.c_uint8), x.shape[0], int(steps), int(batch),
+                                 float(lr), int(seed), C.byref(loss)))
+    return mw, w16, float(loss.value)

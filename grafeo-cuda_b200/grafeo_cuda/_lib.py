@@ -16,6 +16,8 @@ LIB_PATH = os.environ.get("GRAFEO_CUDA_LIBRARY") or os.path.join(_HERE, "libgraf
 u32p = C.POINTER(C.c_uint32)
 i32p = C.POINTER(C.c_int32)
 f32p = C.POINTER(C.c_float)
+u16p = C.POINTER(C.c_uint16)
+u8p = C.POINTER(C.c_uint8)
 
 # name -> (restype, argtypes); mirrors include/grafeo_cuda.h one to one.
 SIGNATURES = {
@@ -146,6 +148,37 @@ SIGNATURES = {
     "gcu_truss_decomposition": (
         C.c_int,
         [C.c_void_p, u32p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_double)],
+    ),
+    "gcu_device_set_schedule": (C.c_int, [C.c_void_p, u16p]),
+    "gcu_schedule_forward": (C.c_int, [C.c_void_p, u16p, f32p, C.c_size_t, f32p]),
+    "gcu_schedule_gradient": (
+        C.c_int,
+        [C.c_void_p, u16p, f32p, f32p, u8p, C.c_size_t, C.POINTER(C.c_double), f32p],
+    ),
+    "gcu_schedule_train": (
+        C.c_int,
+        [
+            C.c_void_p,
+            f32p,
+            u16p,
+            f32p,
+            f32p,
+            u8p,
+            C.c_size_t,
+            C.c_uint32,
+            C.c_uint32,
+            C.c_float,
+            C.c_uint64,
+            C.POINTER(C.c_double),
+        ],
+    ),
+    "gcu_bfs_trace": (
+        C.c_int,
+        [C.c_void_p, C.c_uint32, C.c_uint64, f32p, f32p, u8p, u8p, u8p, C.c_size_t, C.POINTER(C.c_size_t)],
+    ),
+    "gcu_triangle_trace": (
+        C.c_int,
+        [C.c_void_p, f32p, f32p, u8p, u8p, C.c_size_t, C.POINTER(C.c_size_t), C.POINTER(C.c_uint64)],
     ),
     "gcu_edge_list_len": (C.c_size_t, [C.c_void_p]),
     "gcu_edge_list_data": (u32p, [C.c_void_p]),

@@ -261,6 +261,63 @@ GCU_API size_t gcu_edge_list_len(const gcu_edge_list* list);
 GCU_API const uint32_t* gcu_edge_list_data(const gcu_edge_list* list);
 GCU_API void gcu_edge_list_free(gcu_edge_list* list);
 
+/* ---- learned schedule (no reference counterpart: the reference has one
+ * fixed schedule). A 12-32-32-3 network (BF16 weights as uint16_t bit
+ * patterns, FP32 accumulation, ReLU hidden layers) maps the 12 features of a
+ * decision to the predicted log2(microseconds) of three variants: for a BFS
+ * level {push with a warp per frontier vertex, load-balanced push, pull}, for
+ * a DAG out-degree bucket of the triangle count {warp hash table, CTA hash
+ * table, CTA binary search}. Parameter layout: W1[32][12], b1[32], W2[32][32],
+ * b2[32], W3[3][32], b3[3]. The schedule never changes a result. ---- */
+
+#define GCU_SCHEDULE_FEATURES 12
+#define GCU_SCHEDULE_OUTPUTS 3
+#define GCU_SCHEDULE_PARAMS 1571
+
+/* Installs the network on the device for gcu_bfs and gcu_triangle_count
+ * (copied); NULL returns to the fixed rules (the alpha/beta BFS direction
+ * rule and the degree-range intersection buckets), which stay the fallback
+ * wherever the network's prediction is not finite. */
+GCU_API gcu_status gcu_device_set_schedule(gcu_device* dev, const uint16_t* weights);
+
+/* Batched forward pass: out[n][3] for features[n][12]. */
+GCU_API gcu_status gcu_schedule_forward(gcu_device* dev, const uint16_t* weights, const float* features,
+                                        size_t n, float* out);
+/* Masked mean squared error between the predictions and targets[n][3] over
+ * the entries with mask[n][3] != 0, and its gradient w.r.t. the parameters
+ * (grad: GCU_SCHEDULE_PARAMS floats), computed on the device. */
+GCU_API gcu_status gcu_schedule_gradient(gcu_device* dev, const uint16_t* weights, const float* features,
+                                         const float* targets, const uint8_t* mask, size_t n, double* loss,
+                                         float* grad);
+/* Trains on the device: `steps` Adam steps (learning rate lr) on minibatches
+ * of `batch` samples drawn with replacement from the seeded stream. master
+ * (FP32, GCU_SCHEDULE_PARAMS) holds the initial weights and receives the
+ * trained ones; weights receives their BF16 rounding; *final_loss = loss over
+ * all n samples. */
+GCU_API gcu_status gcu_schedule_train(gcu_device* dev, float* master, uint16_t* weights, const float* features,
+                                      const float* targets, const uint8_t* mask, size_t n, uint32_t steps,
+                                      uint32_t batch, float lr, uint64_t seed, double* final_loss);
+
+/* BFS trace from `source`: for every level, the decision's features
+ * (features[level][12]), the device time of every valid variant run from the
+ * same frontier (times_us[level][3], NaN when not valid), the valid-variant
+ * mask, the alpha/beta rule's pick and the variant the traced run continued
+ * with (the rule's pick, or for 3 levels in 10 chosen by explore_seed a
+ * uniformly drawn valid variant). Up to `capacity` levels are written;
+ * *levels = the number of levels traced. The variants must label the same
+ * vertices (GCU_ERR_KERNEL otherwise). */
+GCU_API gcu_status gcu_bfs_trace(gcu_graph* g, uint32_t source, uint64_t explore_seed, float* features,
+                                 float* times_us, uint8_t* valid, uint8_t* fixed_rule, uint8_t* taken,
+                                 size_t capacity, size_t* levels);
+
+/* Triangle-count trace: for every non-empty out-degree bucket of the DAG
+ * (highest first), the features, the device time of every valid
+ * intersection variant (NaN when not valid), the valid mask and the fixed
+ * rule's pick; *total = the triangle count, which every variant of every
+ * bucket must reproduce (GCU_ERR_KERNEL otherwise). At most 33 buckets. */
+GCU_API gcu_status gcu_triangle_trace(gcu_graph* g, float* features, float* times_us, uint8_t* valid,
+                                      uint8_t* fixed_rule, size_t capacity, size_t* buckets, uint64_t* total);
+
 #ifdef __cplusplus
 }
 #endif

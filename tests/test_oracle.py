@@ -167,6 +167,28 @@ def test_oracle_transpose():
     assert o.tolist() == [0, 1, 2, 3, 4] and t.tolist() == [3, 0, 1, 0]
 
 
+def test_schedule_oracle_gradient_matches_central_differences():
+    """The FP64 schedule-network oracle's analytic gradient (against which the
+    GPU gradient kernel is checked) equals central differences of its loss."""
+    from oracle import schedule_mlp as M
+
+    rng = np.random.default_rng(0)
+    p = rng.normal(0, 0.3, M.PARAMS)
+    x = rng.uniform(-1, 2, (50, 12))
+    y = rng.normal(3, 2, (50, 3))
+    m = rng.random((50, 3)) < 0.7
+    _, g = M.loss_and_grad(p, x, y, m)
+    h = 1e-6
+    for i in rng.choice(M.PARAMS, 60, replace=False):
+        e = np.zeros(M.PARAMS)
+        e[i] = h
+        num = (M.loss_and_grad(p + e, x, y, m)[0] - M.loss_and_grad(p - e, x, y, m)[0]) / (2 * h)
+        assert abs(num - g[i]) <= 1e-6 * max(1.0, abs(g[i]))
+    # BF16 rounding is round-to-nearest-even.
+    assert M.bf16_bits(np.array([1.0, 1.00390625, 1.005859375, -2.5], np.float32)).tolist() == [
+        0x3F80, 0x3F80, 0x3F81, 0xC020]
+
+
 def test_oracle_k_truss_round_semantics_on_self_loops():
     """A self-loop inflates first-round support (the reference merges raw lists,
     kernels/k_truss.cu:59-92); the fixpoint is still the maximal k-truss."""
