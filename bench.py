@@ -419,6 +419,35 @@ def secondary(csr, g, dev, args) -> dict:
         "ms": round(tc_ms, 3),
         "triangles": tc["total_triangles"],
     }
+    # The same BFS and triangle count with the learned schedule installed
+    # (the shipped network), against the fixed rules measured above.
+    from grafeo_cuda import schedule as sched
+
+    if os.path.exists(sched.DEFAULT_WEIGHTS):
+        ref_dist = g.bfs_array(int(sources[0]))["distances"]
+        sched.install(dev)
+        try:
+            same = bool(np.array_equal(g.bfs_array(int(sources[0]))["distances"], ref_dist))
+            for s in sources[:3]:
+                g.bfs_array(int(s), copy_result=False)
+            dev.timer_start()
+            for s in sources:
+                g.bfs_array(int(s), copy_result=False)
+            lbfs_ms = dev.timer_stop()
+            tc_l = g.triangle_count()
+            dev.timer_start()
+            for _ in range(reps):
+                tc_l = g.triangle_count()
+            ltc_ms = dev.timer_stop() / reps
+        finally:
+            dev.set_schedule(None)
+        out["learned_schedule"] = {
+            "bfs_gteps": round(total_m / (lbfs_ms / 1e3) / 1e9, 3),
+            "bfs_speedup_vs_alpha_beta": round(bfs_ms / lbfs_ms, 3),
+            "triangle_count_ms": round(ltc_ms, 3),
+            "triangle_speedup_vs_fixed_buckets": round(tc_ms / ltc_ms, 3),
+            "results_identical": same and tc_l["total_triangles"] == tc["total_triangles"],
+        }
     kt = {}
     dev.timer_start()
     for k in range(3, 9):

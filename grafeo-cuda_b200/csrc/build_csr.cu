@@ -129,7 +129,8 @@ __global__ void __launch_bounds__(kBuildThreads) pairs_to_keys_kernel(const uint
 __global__ void __launch_bounds__(kBuildThreads) rmat_keys_kernel(uint64_t state, uint32_t scale, uint64_t m,
                                                                   double a, double ab, double abc,
                                                                   uint64_t* __restrict__ keys,
-                                                                  unsigned long long* __restrict__ count) {
+                                                                  unsigned long long* __restrict__ count,
+                                                                  uint32_t base) {
     GCU_WARP_UNIFORM_LOOP(i, m) {
         const bool valid = i < m;
         uint32_t s = 0, d = 0;
@@ -150,7 +151,7 @@ __global__ void __launch_bounds__(kBuildThreads) rmat_keys_kernel(uint64_t state
                 d = (d << 1) | db;
             }
         }
-        append_undirected(count, keys, valid, s, d);
+        append_undirected(count, keys, valid, s + base, d + base);
     }
 }
 
@@ -202,7 +203,8 @@ __global__ void __launch_bounds__(kBuildThreads) grid_keys_kernel(uint64_t state
 // w drawn from value 2 idx + 1. Self-loops and repeats fall out in the build.
 __global__ void __launch_bounds__(kBuildThreads) ws_keys_kernel(uint64_t state, uint32_t n, uint32_t half, double p,
                                                                 uint64_t* __restrict__ keys,
-                                                                unsigned long long* __restrict__ count) {
+                                                                unsigned long long* __restrict__ count,
+                                                                uint32_t base) {
     const uint64_t total = static_cast<uint64_t>(n) * half;
     GCU_WARP_UNIFORM_LOOP(idx, total) {
         const bool valid = idx < total;
@@ -213,7 +215,7 @@ __global__ void __launch_bounds__(kBuildThreads) ws_keys_kernel(uint64_t state, 
             d = static_cast<uint32_t>((static_cast<uint64_t>(s) + j) % n);
             if (unit_double(stream_at(state, 2 * idx)) < p) d = scale_to(stream_at(state, 2 * idx + 1), n);
         }
-        append_undirected(count, keys, valid, s, d);
+        append_undirected(count, keys, valid, s + base, d + base);
     }
 }
 
@@ -569,7 +571,7 @@ Error generate_graph(DeviceImpl& dev, const GeneratorSpec& spec, GraphImpl& g) {
         case GeneratorSpec::kRmat: {
             const uint64_t m = static_cast<uint64_t>(spec.edge_factor) << spec.scale;
             GCU_LAUNCH(dev, "gen_rmat", rmat_keys_kernel, grid_for(dev, m), kBuildThreads, 0, state, spec.scale, m,
-                       spec.a, spec.a + spec.b, spec.a + spec.b + spec.c, ks.keys.ptr, ks.meta.ptr);
+                       spec.a, spec.a + spec.b, spec.a + spec.b + spec.c, ks.keys.ptr, ks.meta.ptr, 0u);
             break;
         }
         case GeneratorSpec::kErdosRenyi:
@@ -582,7 +584,7 @@ Error generate_graph(DeviceImpl& dev, const GeneratorSpec& spec, GraphImpl& g) {
             break;
         case GeneratorSpec::kWattsStrogatz:
             GCU_LAUNCH(dev, "gen_watts_strogatz", ws_keys_kernel, grid_for(dev, capacity / 2), kBuildThreads, 0,
-                       state, n, spec.k / 2, spec.p, ks.keys.ptr, ks.meta.ptr);
+                       state, n, spec.k / 2, spec.p, ks.keys.ptr, ks.meta.ptr, 0u);
             break;
         case GeneratorSpec::kGeometric:
             GCU_LAUNCH(dev, "gen_geo_pairs", geo_pairs_kernel, grid_for(dev, n), kBuildThreads, 0, pts.ptr,
@@ -603,6 +605,56 @@ Error generate_graph(DeviceImpl& dev, const GeneratorSpec& spec, GraphImpl& g) {
     GCU_TRY(sort_keys(dev, ks.keys.ptr, ks.tmp.ptr, count, id_bits, id_bits, &sorted, &other));
     GCU_TRY(csr_from_sorted_keys(dev, sorted, count, n, g));
     g.symmetric = 1;
+    return ok();
+}
+
+Error generate_union(DeviceImpl& dev, const std::vector<GeneratorSpec>& specs, std::vector<uint32_t>* vbase,
+                     GraphImpl& u) {
+    vbase->assign(specs.size() + 1, 0);
+    uint64_t vertices = 0, capacity = 0;
+    for (size_t i = 0; i < specs.size(); ++i) {
+        const GeneratorSpec& s = specs[i];
+        uint64_t n = 0;
+        if (s.kind == GeneratorSpec::kRmat) {
+            if (s.scale == 0 || s.scale > 31) return export_error("R-MAT scale must be in 1..=31");
+            n = 1ull << s.scale;
+            capacity += 2 * (static_cast<uint64_t>(s.edge_factor) << s.scale);
+        } else if (s.kind == GeneratorSpec::kWattsStrogatz) {
+            if (s.k % 2 != 0) return export_error("Watts-Strogatz k must be even");
+            n = s.n;
+            capacity += 2 * n * (s.k / 2);
+        } else {
+            return kernel_error("a packed batch is generated from R-MAT and Watts-Strogatz graphs only");
+        }
+        (*vbase)[i] = static_cast<uint32_t>(vertices);
+        vertices += n;
+        if (vertices > 0xFFFFFFFEull) return export_error("packed batch has more than 2^32 - 2 vertices");
+    }
+    (*vbase)[specs.size()] = static_cast<uint32_t>(vertices);
+    GCU_TRY(check_capacity(capacity));
+    KeyScratch ks;
+    GCU_TRY(ks.allocate(dev, capacity));
+    for (size_t i = 0; i < specs.size(); ++i) {
+        const GeneratorSpec& s = specs[i];
+        const uint64_t state = host_mix(s.seed + kGamma);
+        const uint32_t base = (*vbase)[i];
+        if (s.kind == GeneratorSpec::kRmat) {
+            const uint64_t m = static_cast<uint64_t>(s.edge_factor) << s.scale;
+            GCU_LAUNCH(dev, "gen_rmat", rmat_keys_kernel, grid_for(dev, m), kBuildThreads, 0, state, s.scale, m, s.a,
+                       s.a + s.b, s.a + s.b + s.c, ks.keys.ptr, ks.meta.ptr, base);
+        } else if (s.n) {
+            GCU_LAUNCH(dev, "gen_watts_strogatz", ws_keys_kernel, grid_for(dev, static_cast<uint64_t>(s.n) * (s.k / 2)),
+                       kBuildThreads, 0, state, s.n, s.k / 2, s.p, ks.keys.ptr, ks.meta.ptr, base);
+        }
+    }
+    uint64_t count = 0, bad = 0;
+    uint32_t maxt = 0;
+    GCU_TRY(ks.read_meta(dev, &count, &bad, &maxt));
+    const uint32_t id_bits = bit_length(vertices > 0 ? vertices - 1 : 0);
+    uint64_t *sorted = nullptr, *other = nullptr;
+    GCU_TRY(sort_keys(dev, ks.keys.ptr, ks.tmp.ptr, count, id_bits, id_bits, &sorted, &other));
+    GCU_TRY(csr_from_sorted_keys(dev, sorted, count, static_cast<uint32_t>(vertices), u));
+    u.symmetric = 1;
     return ok();
 }
 

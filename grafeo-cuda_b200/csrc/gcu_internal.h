@@ -270,6 +270,11 @@ struct GeneratorSpec {
     double avg_degree = 0;                // geometric
 };
 Error generate_graph(DeviceImpl& dev, const GeneratorSpec& spec, GraphImpl& g);
+// Many R-MAT / Watts-Strogatz graphs drawn into one CSR: graph i holds the
+// vertices [vbase[i], vbase[i + 1]) and each graph's lists equal its own
+// generate_graph CSR shifted by vbase[i].
+Error generate_union(DeviceImpl& dev, const std::vector<GeneratorSpec>& specs, std::vector<uint32_t>* vbase,
+                     GraphImpl& u);
 
 // ---------------------------------------------------------------- learned schedule
 
@@ -309,6 +314,42 @@ struct TcTraceBucket {
     uint8_t fixed_rule;
 };
 Error triangle_trace(GraphImpl& g, std::vector<TcTraceBucket>* buckets, uint64_t* total);
+
+// ---------------------------------------------------------------- batched form
+
+// Triangle counting over a union of disjoint graphs: the union's DAG and
+// out-degree buckets with one variant per bucket (learned, or timed once),
+// planned once; batch_tc_launch then only enqueues kernels (capturable), which
+// add every DAG source vertex's triangles into per_vertex[u].
+struct BatchTcPlan;
+Error batch_tc_plan(GraphImpl& u, BatchTcPlan** out, std::string* tuning);
+Error batch_tc_launch(DeviceImpl& dev, BatchTcPlan& p, unsigned long long* per_vertex, uint32_t num_nodes);
+void destroy_batch_tc_plan(BatchTcPlan* p);
+
+// A packed batch of graphs (batch.cu).
+struct BatchImpl;
+void destroy_batch(BatchImpl* b);
+Error batch_generate(DeviceImpl& dev, std::shared_ptr<DeviceImpl> owner, uint32_t num_graphs, uint64_t seed,
+                     BatchImpl** out);
+Error batch_from_csr(DeviceImpl& dev, std::shared_ptr<DeviceImpl> owner, const uint32_t* vbase, size_t num_graphs,
+                     const uint32_t* offsets, size_t n_offsets, const uint32_t* targets, size_t n_targets,
+                     BatchImpl** out);
+uint32_t batch_num_graphs(const BatchImpl& b);
+GraphImpl& batch_union(BatchImpl& b);
+const std::vector<uint32_t>& batch_vertex_base(const BatchImpl& b);
+Error batch_member(BatchImpl& b, uint32_t index, GraphImpl& g);
+Error batch_set_bfs(BatchImpl& b, const uint32_t* sources, uint32_t S, bool keep_distances);
+Error batch_set_ppr(BatchImpl& b, const uint32_t* seeds, uint32_t K, float damping, uint32_t max_iterations,
+                    float tolerance);
+Error batch_run_tc(BatchImpl& b, uint64_t* totals);
+Error batch_run_bfs(BatchImpl& b);
+Error batch_run_ppr(BatchImpl& b);
+Error batch_read_tc(BatchImpl& b, uint64_t* totals);
+Error batch_read_bfs(BatchImpl& b, int32_t* distances, uint32_t* reachable, int32_t* max_depth);
+Error batch_read_ppr(BatchImpl& b, float* ranks, uint32_t* iterations, uint8_t* converged);
+Error batch_capture(BatchImpl& b);
+Error batch_replay(BatchImpl& b);
+std::string batch_tuning(const BatchImpl& b);
 
 }  // namespace gcu
 

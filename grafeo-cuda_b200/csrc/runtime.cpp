@@ -213,6 +213,10 @@ struct gcu_graph {
 struct gcu_edge_list {
     std::vector<uint32_t> data;
 };
+struct gcu_batch {
+    BatchImpl* impl = nullptr;
+    ~gcu_batch() { destroy_batch(impl); }
+};
 
 // ---------------------------------------------------------------- C ABI
 
@@ -737,6 +741,159 @@ GCU_API gcu_status gcu_triangle_trace(gcu_graph* g, float* features, float* time
     *buckets = rec.size();
     *total = t;
     return succeed();
+}
+
+// ---------------------------------------------------------------- batch
+
+static gcu_status on_batch(gcu_batch* b, const std::function<Error(BatchImpl&)>& body) {
+    if (!b || !b->impl) return fail(kernel_error("batch is NULL"));
+    Error e = batch_union(*b->impl).dev->activate();
+    if (e.ok()) e = body(*b->impl);
+    return e.ok() ? succeed() : fail(e);
+}
+
+GCU_API gcu_status gcu_batch_generate(gcu_device* dev, uint32_t num_graphs, uint64_t seed, gcu_batch** out) {
+    if (!out) return fail(kernel_error("out is NULL"));
+    *out = nullptr;
+    return on_device(dev, [&](DeviceImpl& d) {
+        BatchImpl* impl = nullptr;
+        GCU_TRY(batch_generate(d, dev->impl, num_graphs, seed, &impl));
+        *out = new gcu_batch{impl};
+        return ok();
+    });
+}
+
+GCU_API gcu_status gcu_batch_from_csr(gcu_device* dev, const uint32_t* vertex_base, size_t num_graphs,
+                                      const uint32_t* offsets, size_t n_offsets, const uint32_t* targets,
+                                      size_t n_targets, gcu_batch** out) {
+    if (!out) return fail(kernel_error("out is NULL"));
+    *out = nullptr;
+    if (!vertex_base || !offsets || (n_targets && !targets)) return fail(kernel_error("batch CSR pointer is NULL"));
+    if (n_offsets > 0xFFFFFFFFull || n_targets > 0xFFFFFFFFull)
+        return fail(invalid_csr("graph too large for u32 indices: " + std::to_string(n_offsets) + " offsets, " +
+                                std::to_string(n_targets) + " targets"));
+    return on_device(dev, [&](DeviceImpl& d) {
+        BatchImpl* impl = nullptr;
+        GCU_TRY(batch_from_csr(d, dev->impl, vertex_base, num_graphs, offsets, n_offsets, targets, n_targets, &impl));
+        *out = new gcu_batch{impl};
+        return ok();
+    });
+}
+
+GCU_API void gcu_batch_destroy(gcu_batch* b) { delete b; }
+GCU_API uint32_t gcu_batch_num_graphs(const gcu_batch* b) { return b && b->impl ? batch_num_graphs(*b->impl) : 0; }
+GCU_API uint32_t gcu_batch_num_nodes(const gcu_batch* b) {
+    return b && b->impl ? batch_union(*b->impl).num_nodes : 0;
+}
+GCU_API uint32_t gcu_batch_num_edges(const gcu_batch* b) {
+    return b && b->impl ? batch_union(*b->impl).num_edges : 0;
+}
+
+GCU_API gcu_status gcu_batch_vertex_base(const gcu_batch* b, uint32_t* vertex_base) {
+    if (!b || !b->impl || !vertex_base) return fail(kernel_error("gcu_batch_vertex_base: NULL argument"));
+    const auto& v = batch_vertex_base(*b->impl);
+    std::copy(v.begin(), v.end(), vertex_base);
+    return succeed();
+}
+
+GCU_API gcu_status gcu_batch_copy_csr(const gcu_batch* b, uint32_t* offsets, uint32_t* targets) {
+    if (!b || !b->impl) return fail(kernel_error("batch is NULL"));
+    GraphImpl& u = batch_union(*b->impl);
+    if (!offsets || (u.num_edges && !targets)) return fail(kernel_error("gcu_batch_copy_csr: NULL argument"));
+    DeviceImpl& d = *u.dev;
+    Error e = d.activate();
+    if (!e.ok()) return fail(e);
+    cudaError_t c = cudaMemcpyAsync(offsets, u.offsets.ptr, 4 * (static_cast<size_t>(u.num_nodes) + 1),
+                                    cudaMemcpyDeviceToHost, d.stream);
+    if (c == cudaSuccess && u.num_edges)
+        c = cudaMemcpyAsync(targets, u.targets.ptr, 4 * static_cast<size_t>(u.num_edges), cudaMemcpyDeviceToHost,
+                            d.stream);
+    if (c != cudaSuccess) return fail(driver_error(c, "copy CSR to host"));
+    e = d.sync();
+    return e.ok() ? succeed() : fail(e);
+}
+
+GCU_API gcu_status gcu_batch_member(gcu_batch* b, uint32_t index, gcu_graph** out) {
+    if (!out) return fail(kernel_error("out is NULL"));
+    *out = nullptr;
+    return on_batch(b, [&](BatchImpl& bi) {
+        auto g = std::make_unique<GraphImpl>();
+        g->dev = batch_union(bi).dev;
+        GCU_TRY(batch_member(bi, index, *g));
+        *out = new gcu_graph{std::move(g)};
+        return ok();
+    });
+}
+
+GCU_API gcu_status gcu_batch_triangle_count(gcu_batch* b, uint64_t* totals, double* seconds) {
+    WallTimer wall;
+    if (!totals) return fail(kernel_error("totals is NULL"));
+    gcu_status s = on_batch(b, [&](BatchImpl& bi) { return batch_run_tc(bi, totals); });
+    if (s == GCU_OK && seconds) *seconds = wall.seconds();
+    return s;
+}
+
+GCU_API gcu_status gcu_batch_set_bfs_sources(gcu_batch* b, const uint32_t* sources, uint32_t S, int keep_distances) {
+    if (!sources) return fail(kernel_error("sources is NULL"));
+    return on_batch(b, [&](BatchImpl& bi) { return batch_set_bfs(bi, sources, S, keep_distances != 0); });
+}
+
+GCU_API gcu_status gcu_batch_bfs(gcu_batch* b, int32_t* distances, uint32_t* reachable, int32_t* max_depth,
+                                 double* seconds) {
+    WallTimer wall;
+    gcu_status s = on_batch(b, [&](BatchImpl& bi) {
+        GCU_TRY(batch_run_bfs(bi));
+        return batch_read_bfs(bi, distances, reachable, max_depth);
+    });
+    if (s == GCU_OK && seconds) *seconds = wall.seconds();
+    return s;
+}
+
+GCU_API gcu_status gcu_batch_set_pagerank_seeds(gcu_batch* b, const uint32_t* seeds, uint32_t K, float damping,
+                                                uint32_t max_iterations, float tolerance) {
+    if (!seeds) return fail(kernel_error("seeds is NULL"));
+    return on_batch(b,
+                    [&](BatchImpl& bi) { return batch_set_ppr(bi, seeds, K, damping, max_iterations, tolerance); });
+}
+
+GCU_API gcu_status gcu_batch_personalized_pagerank(gcu_batch* b, float* ranks, uint32_t* iterations,
+                                                   uint8_t* converged, double* seconds) {
+    WallTimer wall;
+    gcu_status s = on_batch(b, [&](BatchImpl& bi) {
+        GCU_TRY(batch_run_ppr(bi));
+        return batch_read_ppr(bi, ranks, iterations, converged);
+    });
+    if (s == GCU_OK && seconds) *seconds = wall.seconds();
+    return s;
+}
+
+GCU_API gcu_status gcu_batch_capture(gcu_batch* b) {
+    return on_batch(b, [&](BatchImpl& bi) { return batch_capture(bi); });
+}
+
+GCU_API gcu_status gcu_batch_replay(gcu_batch* b) {
+    return on_batch(b, [&](BatchImpl& bi) { return batch_replay(bi); });
+}
+
+GCU_API gcu_status gcu_batch_results(gcu_batch* b, uint64_t* triangles, int32_t* distances, uint32_t* reachable,
+                                     int32_t* max_depth, float* ranks, uint32_t* iterations, uint8_t* converged) {
+    return on_batch(b, [&](BatchImpl& bi) {
+        GCU_TRY(batch_union(bi).dev->sync());
+        if (triangles) GCU_TRY(batch_read_tc(bi, triangles));
+        GCU_TRY(batch_read_bfs(bi, distances, reachable, max_depth));
+        return batch_read_ppr(bi, ranks, iterations, converged);
+    });
+}
+
+GCU_API size_t gcu_batch_tuning(const gcu_batch* b, char* buf, size_t buflen) {
+    if (!b || !b->impl) return 0;
+    const std::string s = batch_tuning(*b->impl);
+    if (buf && buflen) {
+        const size_t n = std::min(buflen - 1, s.size());
+        std::memcpy(buf, s.data(), n);
+        buf[n] = '\0';
+    }
+    return s.size() + 1;
 }
 
 GCU_API size_t gcu_edge_list_len(const gcu_edge_list* list) { return list ? list->data.size() / 2 : 0; }

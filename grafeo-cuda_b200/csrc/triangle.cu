@@ -127,6 +127,7 @@ struct CountSink {
     unsigned long long* total;
     unsigned long long count;
     __device__ __forceinline__ void hit(uint32_t, uint32_t, uint32_t, uint32_t) { ++count; }
+    __device__ __forceinline__ void end_vertex(uint32_t) {}
     __device__ __forceinline__ void finish() {
         unsigned long long c = warp_sum(count);
         if (lane_id() == 0 && c) atomicAdd(total, c);
@@ -418,6 +419,114 @@ Error triangle_count(GraphImpl& g, bool oriented, uint64_t* total) {
 
 Error triangle_trace(GraphImpl& g, std::vector<TcTraceBucket>* buckets, uint64_t* total) {
     return triangle_count_ex(g, false, total, buckets);
+}
+
+// ---------------------------------------------------------------- batched form
+
+namespace {
+
+// Triangles per DAG source vertex: each warp adds its lanes' count for u.
+struct VertexCountSink {
+    static constexpr bool kNeedsPos = false;
+    unsigned long long* per_vertex;
+    unsigned long long count;
+    __device__ __forceinline__ void hit(uint32_t, uint32_t, uint32_t, uint32_t) { ++count; }
+    __device__ __forceinline__ void end_vertex(uint32_t u) {
+        const unsigned long long c = warp_sum(count);
+        if (lane_id() == 0 && c) atomicAdd(per_vertex + u, c);
+        count = 0;
+    }
+    __device__ __forceinline__ void finish() {}
+};
+
+}  // namespace
+
+struct BatchTcPlan {
+    DeviceBuffer<uint32_t> dag_offsets, dag_targets;
+    uint32_t m = 0;
+    BucketPlan buckets;
+    int variant[kBuckets] = {};
+    DeviceBuffer<uint32_t> next;  // handout counter per bucket
+};
+
+void destroy_batch_tc_plan(BatchTcPlan* p) { delete p; }
+
+Error batch_tc_plan(GraphImpl& u, BatchTcPlan** out, std::string* tuning) {
+    DeviceImpl& dev = *u.dev;
+    auto p = std::make_unique<BatchTcPlan>();
+    GCU_TRY(build_dag(u, true, nullptr, &p->dag_offsets, &p->dag_targets, nullptr, &p->m));
+    DegreeStats stats;
+    if (dev.schedule) GCU_TRY(degree_stats(u, &stats));
+    GCU_TRY(plan_buckets(dev, p->dag_offsets.ptr, u.num_nodes, 2, p->m, stats, false, p->buckets));
+    GCU_TRY(p->next.allocate(dev, kBuckets * kSchedOut));
+    // Variant per bucket: the learned schedule's pick when one is installed,
+    // else the fastest valid variant timed once on this batch (autotune).
+    DeviceBuffer<unsigned long long> scratch;
+    GCU_TRY(scratch.allocate(dev, std::max<uint32_t>(u.num_nodes, 1)));
+    GCU_CUDA(cudaMemsetAsync(p->next.ptr, 0, sizeof(uint32_t) * kBuckets * kSchedOut, dev.stream), "memset");
+    cudaEvent_t ev[2 * kSchedOut];
+    for (auto& e : ev) GCU_CUDA(cudaEventCreate(&e), "cudaEventCreate");
+    struct Guard {
+        cudaEvent_t* e;
+        ~Guard() {
+            for (int i = 0; i < 2 * kSchedOut; ++i) cudaEventDestroy(e[i]);
+        }
+    } guard{ev};
+    std::string json = "{";
+    for (int c = kBuckets - 1; c >= 0; --c) {
+        if (p->buckets.host_counts[c] == 0) continue;
+        const unsigned valid = bucket_valid(c);
+        int pick = bucket_fixed(c);
+        float best = 0.f;
+        const int learned = p->buckets.host_choices[c];
+        std::string how;
+        if (learned >= 0 && ((valid >> learned) & 1u)) {
+            pick = learned;
+            how = "learned";
+        } else {
+            bool first = true;
+            for (int v = 0; v < kSchedOut; ++v) {
+                if (!((valid >> v) & 1u)) continue;
+                GCU_CUDA(cudaEventRecord(ev[2 * v], dev.stream), "cudaEventRecord");
+                GCU_TRY(launch_bucket(dev, p->dag_offsets.ptr, p->dag_targets.ptr, p->buckets, c, v,
+                                      p->next.ptr + c * kSchedOut + v, VertexCountSink{scratch.ptr, 0}));
+                GCU_CUDA(cudaEventRecord(ev[2 * v + 1], dev.stream), "cudaEventRecord");
+            }
+            GCU_TRY(dev.sync());
+            for (int v = 0; v < kSchedOut; ++v) {
+                if (!((valid >> v) & 1u)) continue;
+                float ms = 0.f;
+                GCU_CUDA(cudaEventElapsedTime(&ms, ev[2 * v], ev[2 * v + 1]), "cudaEventElapsedTime");
+                if (first || ms < best) {
+                    best = ms;
+                    pick = v;
+                    first = false;
+                }
+            }
+            how = "timed";
+        }
+        p->variant[c] = pick;
+        if (json.size() > 1) json += ", ";
+        json += "\"" + std::to_string(c) + "\": {\"vertices\": " + std::to_string(p->buckets.host_counts[c]) +
+                ", \"variant\": " + std::to_string(pick) + ", \"by\": \"" + how + "\"}";
+    }
+    json += "}";
+    if (tuning) *tuning = json;
+    GCU_TRY(dev.sync());
+    *out = p.release();
+    return ok();
+}
+
+Error batch_tc_launch(DeviceImpl& dev, BatchTcPlan& p, unsigned long long* per_vertex, uint32_t num_nodes) {
+    GCU_CUDA(cudaMemsetAsync(per_vertex, 0, sizeof(unsigned long long) * std::max<uint32_t>(num_nodes, 1), dev.stream),
+             "memset");
+    GCU_CUDA(cudaMemsetAsync(p.next.ptr, 0, sizeof(uint32_t) * kBuckets, dev.stream), "memset");
+    for (int c = kBuckets - 1; c >= 0; --c) {
+        if (p.buckets.host_counts[c] == 0) continue;
+        GCU_TRY(launch_bucket(dev, p.dag_offsets.ptr, p.dag_targets.ptr, p.buckets, c, p.variant[c], p.next.ptr + c,
+                              VertexCountSink{per_vertex, 0}));
+    }
+    return ok();
 }
 
 }  // namespace gcu

@@ -228,7 +228,9 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_kernel(const uint32_t
 
 // ---------------------------------------------------------------- bucket kernels
 // The same intersections over an explicit vertex list (one out-degree bucket
-// of a DAG), so that a schedule can pick the variant per bucket.
+// of a DAG), so that a schedule can pick the variant per bucket. Their sinks
+// also get end_vertex(u) from every warp that worked on u, once it is done
+// with u (all 32 lanes call it).
 
 // Warp per listed vertex; a shared hash table per warp for out-lists of at
 // most kWarpMaxDeg entries, binary search in global memory beyond (the
@@ -273,6 +275,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_warp_list_kernel(const ui
                         return use_table ? hash_find<kPos>(keys, pos, bits, w) : sorted_find(ulist, du, w);
                     },
                     [&](uint32_t pv, uint32_t pw, uint32_t evw) { sink.hit(s, pv, pw, evw); });
+            sink.end_vertex(u);
         }
     }
     sink.finish();
@@ -318,6 +321,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_list_kernel(const uin
                     return use_table ? hash_find<kPos>(s_keys, pos, bits, w) : sorted_find(ulist, du, w);
                 },
                 [&](uint32_t pv, uint32_t pw, uint32_t evw) { sink.hit(s, pv, pw, evw); });
+        sink.end_vertex(u);
         __syncthreads();  // the table and s_item are reused by the next list
     }
     sink.finish();

@@ -538,6 +538,9 @@ class GpuGraph:
                 "total_triangles": int(total.value)}
 
 
+from .batch import GpuBatch  # noqa: E402  (needs the classes above)
+
+
 # ---------------------------------------------------------------- schedule network kernels
 
 

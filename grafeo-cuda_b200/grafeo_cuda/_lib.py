@@ -149,6 +149,33 @@ SIGNATURES = {
         C.c_int,
         [C.c_void_p, u32p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_double)],
     ),
+    "gcu_batch_generate": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "gcu_batch_from_csr": (
+        C.c_int,
+        [C.c_void_p, u32p, C.c_size_t, u32p, C.c_size_t, u32p, C.c_size_t, C.POINTER(C.c_void_p)],
+    ),
+    "gcu_batch_destroy": (None, [C.c_void_p]),
+    "gcu_batch_num_graphs": (C.c_uint32, [C.c_void_p]),
+    "gcu_batch_num_nodes": (C.c_uint32, [C.c_void_p]),
+    "gcu_batch_num_edges": (C.c_uint32, [C.c_void_p]),
+    "gcu_batch_vertex_base": (C.c_int, [C.c_void_p, u32p]),
+    "gcu_batch_copy_csr": (C.c_int, [C.c_void_p, u32p, u32p]),
+    "gcu_batch_member": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "gcu_batch_triangle_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
+    "gcu_batch_set_bfs_sources": (C.c_int, [C.c_void_p, u32p, C.c_uint32, C.c_int]),
+    "gcu_batch_bfs": (C.c_int, [C.c_void_p, i32p, u32p, i32p, C.POINTER(C.c_double)]),
+    "gcu_batch_set_pagerank_seeds": (
+        C.c_int,
+        [C.c_void_p, u32p, C.c_uint32, C.c_float, C.c_uint32, C.c_float],
+    ),
+    "gcu_batch_personalized_pagerank": (C.c_int, [C.c_void_p, f32p, u32p, u8p, C.POINTER(C.c_double)]),
+    "gcu_batch_capture": (C.c_int, [C.c_void_p]),
+    "gcu_batch_replay": (C.c_int, [C.c_void_p]),
+    "gcu_batch_results": (
+        C.c_int,
+        [C.c_void_p, C.POINTER(C.c_uint64), i32p, u32p, i32p, f32p, u32p, u8p],
+    ),
+    "gcu_batch_tuning": (C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "gcu_device_set_schedule": (C.c_int, [C.c_void_p, u16p]),
     "gcu_schedule_forward": (C.c_int, [C.c_void_p, u16p, f32p, C.c_size_t, f32p]),
     "gcu_schedule_gradient": (

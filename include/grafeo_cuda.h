@@ -270,6 +270,68 @@ GCU_API void gcu_edge_list_free(gcu_edge_list* list);
  * table, CTA binary search}. Parameter layout: W1[32][12], b1[32], W2[32][32],
  * b2[32], W3[3][32], b3[3]. The schedule never changes a result. ---- */
 
+/* ---- batched form (no reference counterpart: the reference runs one graph
+ * per call). Many graphs packed into one CSR: graph i owns the vertices
+ * [vertex_base[i], vertex_base[i + 1]) of a union CSR whose targets are union
+ * ids, and no edge leaves its graph. Triangle counts, BFS from S sources per
+ * graph and personalised PageRank from K seeds per graph run as persistent
+ * kernels over all graphs at once; gcu_batch_capture records the three into
+ * one CUDA graph that gcu_batch_replay launches. Results equal the per-graph
+ * calls (gcu_triangle_count, gcu_bfs, gcu_personalized_pagerank with the same
+ * seeds), which gcu_batch_member makes possible for comparison. ---- */
+
+typedef struct gcu_batch gcu_batch;
+
+/* The synthetic corpus: graph i is R-MAT (scale U{8..16}, edge factor
+ * U{8..32}, a, b, c = 0.57, 0.19, 0.19) or Watts-Strogatz (n U{256..65536},
+ * k = 10, p = 0.1) with equal odds, drawn from (seed, i) and generated on the
+ * device. */
+GCU_API gcu_status gcu_batch_generate(gcu_device* dev, uint32_t num_graphs, uint64_t seed, gcu_batch** out);
+/* A union CSR from the host, validated like gcu_graph_from_csr plus the
+ * no-edge-leaves-its-graph rule (GCU_ERR_KERNEL). */
+GCU_API gcu_status gcu_batch_from_csr(gcu_device* dev, const uint32_t* vertex_base, size_t num_graphs,
+                                      const uint32_t* offsets, size_t n_offsets, const uint32_t* targets,
+                                      size_t n_targets, gcu_batch** out);
+GCU_API void gcu_batch_destroy(gcu_batch* b);
+GCU_API uint32_t gcu_batch_num_graphs(const gcu_batch* b);
+GCU_API uint32_t gcu_batch_num_nodes(const gcu_batch* b);
+GCU_API uint32_t gcu_batch_num_edges(const gcu_batch* b);
+/* vertex_base: num_graphs + 1 values. */
+GCU_API gcu_status gcu_batch_vertex_base(const gcu_batch* b, uint32_t* vertex_base);
+/* The union CSR copied back (num_nodes + 1 offsets, num_edges targets). */
+GCU_API gcu_status gcu_batch_copy_csr(const gcu_batch* b, uint32_t* offsets, uint32_t* targets);
+/* Member `index` as a separate device graph with local ids. */
+GCU_API gcu_status gcu_batch_member(gcu_batch* b, uint32_t index, gcu_graph** out);
+
+/* Triangles of every graph (totals: num_graphs values). */
+GCU_API gcu_status gcu_batch_triangle_count(gcu_batch* b, uint64_t* totals, double* seconds);
+/* Sets the BFS sources: sources[g * S + k] is source k of graph g (local id),
+ * 1 <= S <= 32. keep_distances = 0 skips the per-vertex distances. */
+GCU_API gcu_status gcu_batch_set_bfs_sources(gcu_batch* b, const uint32_t* sources, uint32_t S,
+                                             int keep_distances);
+/* Runs the BFS; distances (S * num_nodes, source-major: distances[k *
+ * num_nodes + v] for union vertex v; may be NULL), reachable and max_depth
+ * (num_graphs * S each, graph-major; may be NULL) as gcu_bfs gives them. */
+GCU_API gcu_status gcu_batch_bfs(gcu_batch* b, int32_t* distances, uint32_t* reachable, int32_t* max_depth,
+                                 double* seconds);
+/* Sets the personalised PageRank seeds: seeds[g * K + k] (local ids). */
+GCU_API gcu_status gcu_batch_set_pagerank_seeds(gcu_batch* b, const uint32_t* seeds, uint32_t K, float damping,
+                                                uint32_t max_iterations, float tolerance);
+/* Runs it; ranks (num_nodes, may be NULL), iterations and converged
+ * (num_graphs each, may be NULL). */
+GCU_API gcu_status gcu_batch_personalized_pagerank(gcu_batch* b, float* ranks, uint32_t* iterations,
+                                                   uint8_t* converged, double* seconds);
+/* Plans, autotunes and captures triangles + BFS + PageRank into one CUDA
+ * graph; gcu_batch_replay enqueues it on the device stream (asynchronous);
+ * gcu_batch_results synchronizes and copies any of the results (NULL skips). */
+GCU_API gcu_status gcu_batch_capture(gcu_batch* b);
+GCU_API gcu_status gcu_batch_replay(gcu_batch* b);
+GCU_API gcu_status gcu_batch_results(gcu_batch* b, uint64_t* triangles, int32_t* distances, uint32_t* reachable,
+                                     int32_t* max_depth, float* ranks, uint32_t* iterations, uint8_t* converged);
+/* JSON of the autotuned choices (variant per bucket, CTA sizes with their
+ * timings); returns the length, writes up to buflen bytes. */
+GCU_API size_t gcu_batch_tuning(const gcu_batch* b, char* buf, size_t buflen);
+
 #define GCU_SCHEDULE_FEATURES 12
 #define GCU_SCHEDULE_OUTPUTS 3
 #define GCU_SCHEDULE_PARAMS 1571

@@ -42,9 +42,16 @@ def run_torchrun(args, env_extra=None, timeout=300):
     env["CUDA_VISIBLE_DEVICES"] = ""
     if env_extra:
         env.update(env_extra)
-    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
-           "--master-addr=127.0.0.1", f"--master-port={free_port()}"] + args
-    return subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout, cwd=ROOT)
+    # A port picked free can be taken again before the rendezvous binds it:
+    # retry on a fresh port when the launcher itself fails.
+    for attempt in range(3):
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
+               "--master-addr=127.0.0.1", f"--master-port={free_port()}"] + args
+        r = subprocess.run(cmd, capture_output=True, text=True, env=env, timeout=timeout, cwd=ROOT)
+        if r.returncode == 0 or not any(s in r.stderr for s in ("EADDRINUSE", "address already in use",
+                                                                 "RendezvousConnectionError", "DistNetworkError")):
+            return r
+    return r
 
 
 def test_dist_max_and_sum_over_two_gloo_ranks(tmp_path):
