@@ -57,6 +57,11 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--no-secondary", action="store_true", help="skip BFS/TC/k-truss lines")
+    ap.add_argument("--suite", action="store_true",
+                    help="instead of the headline: all four algorithms on R-MAT 22 and Erdos-Renyi 2^22, and "
+                         "R-MAT 24 (directed PageRank with 3%% dangling vertices and its error, truss "
+                         "decomposition, BFS and triangles with the learned schedule against the fixed rules); "
+                         "one JSON document")
     return ap.parse_args()
 
 
@@ -381,7 +386,7 @@ def cpu_pagerank_sample(csr, B: int, seconds: float) -> dict:
     }
 
 
-def secondary(csr, g, dev, args) -> dict:
+def secondary(csr, g, dev, args, k_truss: bool = True) -> dict:
     """BFS, triangle counting and k-truss on the resident graph (device time)."""
     out = {}
     V, E = csr.num_nodes, csr.num_edges
@@ -448,6 +453,8 @@ def secondary(csr, g, dev, args) -> dict:
             "triangle_speedup_vs_fixed_buckets": round(tc_ms / ltc_ms, 3),
             "results_identical": same and tc_l["total_triangles"] == tc["total_triangles"],
         }
+    if not k_truss:
+        return out
     kt = {}
     dev.timer_start()
     for k in range(3, 9):
@@ -461,6 +468,95 @@ def secondary(csr, g, dev, args) -> dict:
         "ms_total": round(kt_ms, 2),
         "per_k": kt,
     }
+    return out
+
+
+# ---------------------------------------------------------------- suite (configurations at scale)
+
+
+def pagerank_gbs(g, dev, V: int, E: int, iterations: int = PR_ITERATIONS) -> dict:
+    g.pagerank_array(DAMPING, iterations, 0.0, copy_result=False)
+    dev.timer_start()
+    g.pagerank_array(DAMPING, iterations, 0.0, copy_result=False)
+    ms = dev.timer_stop()
+    return {"metric": "PageRank iteration GB/s (4E+12V+4 bytes per iteration)",
+            "value": round(pr_bytes(V, E) * iterations / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
+            "ms_per_iteration": round(ms / iterations, 4)}
+
+
+def directed_dangling_copy(csr, fraction: float, seed: int):
+    """The directed copy of a symmetric CSR in which a seeded uniform
+    `fraction` of the vertices lose their out-edges (they become dangling)."""
+    V = csr.num_nodes
+    rng = np.random.default_rng(seed)
+    drop = np.zeros(V, dtype=bool)
+    drop[rng.choice(V, size=int(round(fraction * V)), replace=False)] = True
+    deg = np.diff(csr.offsets).astype(np.int64)
+    keep_rows = ~drop
+    offsets = np.zeros(V + 1, dtype=np.int64)
+    np.cumsum(np.where(keep_rows, deg, 0), out=offsets[1:])
+    targets = csr.targets[np.repeat(keep_rows, deg)]
+    return offsets.astype(np.uint32), targets, int(drop.sum())
+
+
+def run_suite(args) -> dict:
+    import grafeo_cuda as G
+    from oracle import oracle as O
+
+    dev = G.GpuDevice(0)
+    out = {"suite": "four algorithms at scale; learned schedule against the fixed rules", "device": dev.name}
+    graphs = (
+        ("rmat22", "R-MAT scale 22, edge factor 16, a=0.57 b=0.19 c=0.19, seed 2",
+         lambda: G.GpuGraph.generate_rmat(dev, 22, EDGE_FACTOR, *RMAT_ABC, seed=2)),
+        ("er22", "Erdos-Renyi G(n = 4,194,304, 16n pairs -> average degree ~32), seed 3",
+         lambda: G.GpuGraph.generate_erdos_renyi(dev, 1 << 22, 16 << 22, seed=3)),
+    )
+    for name, what, make in graphs:
+        g = make()
+        csr = g.to_csr()
+        block = {"graph": what, "vertices": csr.num_nodes, "csr_entries": csr.num_edges,
+                 "pagerank": pagerank_gbs(g, dev, csr.num_nodes, csr.num_edges)}
+        block.update(secondary(csr, g, dev, args))
+        out[name] = block
+        del g
+    # R-MAT 24, seed 5.
+    t0 = time.time()
+    g = G.GpuGraph.generate_rmat(dev, 24, EDGE_FACTOR, *RMAT_ABC, seed=5)
+    dev.synchronize()
+    gen_s = time.time() - t0
+    csr = g.to_csr()
+    V, E = csr.num_nodes, csr.num_edges
+    s24 = {"graph": "R-MAT scale 24, edge factor 16, a=0.57 b=0.19 c=0.19, seed 5", "vertices": V,
+           "csr_entries": E, "device_generation_s": round(gen_s, 3)}
+    # Directed copy with 3 % dangling vertices: PageRank to tol 1e-7 (<= 100 iterations).
+    doff, dtgt, ndrop = directed_dangling_copy(csr, 0.03, seed=5)
+    gd = G.GpuGraph.from_csr(doff, dtgt, dev)
+    gd.pagerank_directed(DAMPING, 2, 0.0)  # builds the transpose plan (not timed)
+    dev.timer_start()
+    pr = gd.pagerank_directed(DAMPING, 100, 1e-7)
+    pr_ms = dev.timer_stop()
+    t0 = time.perf_counter()
+    ref = O.pagerank_directed(doff, dtgt, DAMPING, pr["iterations"], 0.0)
+    ref_s = time.perf_counter() - t0
+    err = np.asarray(pr["ranks"], dtype=np.float64) - ref["ranks"]
+    s24["pagerank_directed"] = {
+        "dangling_vertices": ndrop, "csr_entries": int(len(dtgt)), "damping": DAMPING, "tolerance": 1e-7,
+        "iterations": pr["iterations"], "converged": pr["converged"], "device_ms": round(pr_ms, 2),
+        "ms_per_iteration": round(pr_ms / max(pr["iterations"], 1), 4),
+        "l1_error_vs_fp64_oracle": float(np.abs(err).sum()), "linf_error_vs_fp64_oracle": float(np.abs(err).max()),
+        "oracle": f"FP64 power iteration, same {pr['iterations']} iterations, {O.num_threads()} threads, {ref_s:.1f} s",
+    }
+    del gd
+    # Truss decomposition (every k up to the maximum trussness).
+    dev.timer_start()
+    td = g.truss_decomposition(copy_result=False)
+    td_ms = dev.timer_stop()
+    s24["truss_decomposition"] = {"max_trussness": td["max_trussness"], "rounds": td["rounds"],
+                                  "device_ms": round(td_ms, 1),
+                                  "edges_per_s": round((E // 2) / (td_ms / 1e3), 1)}
+    # BFS and triangles, with the learned schedule against the fixed rules.
+    s24.update(secondary(csr, g, dev, args, k_truss=False))
+    out["rmat24"] = s24
     return out
 
 
@@ -514,6 +610,9 @@ def run_reference(args, d: Dist) -> dict | None:
 
 def main():
     args = parse_args()
+    if args.suite:
+        print(json.dumps(run_suite(args)), flush=True)
+        return
     d = Dist()
     try:
         line = run_reference(args, d) if args.impl == "reference" else run_ours(args, d)
