@@ -24,12 +24,17 @@
 //    carry. Rows of 4096 or more entries are split into 4096-entry segments,
 //    one block each, and their partial sums are added in segment order by the
 //    finishing kernel.
+//  * Work blocks (a long-row segment, or 2 rows per lane group of one class)
+//    are grouped into chunks of about equal estimated work, ordered heaviest
+//    first, and the persistent CTAs take chunks from a counter, so a CTA that
+//    drew heavy rows takes fewer.
 //  * Row sums: FP32 Kahan sums per lane, FP64 across lanes (shuffle tree) and
 //    across segments. Epilogue per row v: r'[v] = (1-d)/N + d (sum +
-//    dangling/N); |r' - r| and the dangling mass of r' go to FP64 per-block
-//    partials that the last block of the finishing kernel reduces in a fixed
-//    order (deterministic, no float atomics); c'[v] = r'[v] / deg(v) is
-//    written for the next iteration.
+//    dangling/N); |r' - r| and the dangling mass of r' are summed as 64-bit
+//    fixed-point integers (2^-62 units) per CTA and reduced by the last block
+//    of the finishing kernel: integer sums do not depend on the order, so the
+//    result is deterministic whichever CTA took which chunk (no float
+//    atomics); c'[v] = r'[v] / deg(v) is written for the next iteration.
 //  * The iteration loop stays on the device: each kernel reads a `done` flag
 //    first, so the host queues iterations ahead and polls the flag once per
 //    chunk instead of syncing every iteration.
@@ -95,8 +100,11 @@ struct PageRankPlan {
     DeviceBuffer<float> ranks;         // 2 * V: ping-pong, relabelled order
     DeviceBuffer<float> contrib;       // 2 * V: ping-pong, relabelled order
     DeviceBuffer<float> ranks_out;     // V: result in original order
-    DeviceBuffer<double> row_partials; // 2 per block of the row kernel
-    DeviceBuffer<double> fin_partials; // 2 per block of the finishing kernel
+    DeviceBuffer<unsigned long long> row_partials; // 2 fixed-point sums per CTA of the row kernel
+    DeviceBuffer<unsigned long long> fin_partials; // 2 per block of the finishing kernel
+    DeviceBuffer<uint2> chunks;        // [first, end) block ranges, heaviest first
+    uint32_t nchunks = 0;
+    DeviceBuffer<uint32_t> next_chunk; // dispatch counter of the row kernel (reset by the finishing kernel)
     DeviceBuffer<PrState> state;
     PrState* host_state = nullptr;     // pinned
 };
@@ -281,6 +289,17 @@ __device__ __forceinline__ void pr_finish_row(uint32_t v, double sum, uint32_t r
     if (deg == 0) dangle += static_cast<double>(r);
 }
 
+// The L1 change and the dangling mass are summed as 64-bit fixed-point
+// integers (units of 2^-62; every term lies in [0, 2] and so does every sum):
+// integer addition is associative, so the totals do not depend on which CTA
+// handled which rows, and the dynamic block handout stays deterministic.
+__device__ __forceinline__ unsigned long long to_fixed(double x) {
+    return __double2ull_rz(x * 4611686018427387904.0);
+}
+__device__ __forceinline__ double from_fixed(unsigned long long q) {
+    return static_cast<double>(q) * (1.0 / 4611686018427387904.0);
+}
+
 __device__ __forceinline__ void kahan_add(float& acc, float& comp, float x) {
     const float y = x - comp;
     const float t = acc + y;
@@ -294,21 +313,32 @@ __device__ __forceinline__ double group_sum(double v, uint32_t log2g) {
     return v;
 }
 
-// Persistent: each CTA walks the schedule's work blocks b = blockIdx.x,
-// blockIdx.x + gridDim.x, ... (a fixed assignment, so the per-CTA partial sums
-// are deterministic). 8 CTAs of 256 threads per SM (32 registers).
+// Persistent: each CTA takes chunks of consecutive work blocks from a counter
+// (chunks of about equal estimated work, the heaviest first), so a CTA that
+// drew heavy rows takes fewer chunks. 8 CTAs of 256 threads per SM.
 __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
     const uint32_t* __restrict__ poff, const uint32_t* __restrict__ ptgt, const float* __restrict__ rank_in,
     const float* __restrict__ contrib_in, float* __restrict__ rank_out, float* __restrict__ contrib_out,
     const uint32_t* __restrict__ outdeg, const float* __restrict__ tele, uint32_t V, double base, double damp,
     const PrState* __restrict__ state, const PrSchedule sched,
-    const uint2* __restrict__ units, double* __restrict__ seg_partial, double* __restrict__ row_partials) {
+    const uint2* __restrict__ units, double* __restrict__ seg_partial,
+    unsigned long long* __restrict__ row_partials, const uint2* __restrict__ chunks, uint32_t nchunks,
+    uint32_t* __restrict__ next_chunk) {
     if (state->done) return;
     __shared__ double scratch[32];
+    __shared__ uint32_t s_chunk[2];
     const double dangling = state->dangling;
     const double spread = dangling / static_cast<double>(V);
-    double my_diff = 0.0, my_dangle = 0.0;
-    for (uint32_t b = blockIdx.x; b < sched.total_blocks; b += gridDim.x) {
+    unsigned long long my_diff = 0, my_dangle = 0;
+    for (uint32_t trip = 0;; ++trip) {
+    // Two slots: a slot is rewritten two trips later, after every thread has
+    // passed the barrier of the trip in between.
+    if (threadIdx.x == 0) s_chunk[trip & 1] = atomicAdd(next_chunk, 1u);
+    __syncthreads();
+    const uint32_t ci = s_chunk[trip & 1];
+    if (ci >= nchunks) break;
+    const uint2 chunk = chunks[ci];
+    for (uint32_t b = chunk.x; b < chunk.y; ++b) {
     uint32_t pi = 0;
     while (pi + 1 < sched.nphases && sched.phase[pi + 1].first_block <= b) ++pi;
     const PrPhase ph = sched.phase[pi];
@@ -384,19 +414,30 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
         for (int q = 0; q < kRowsPerGroup; ++q) {
             const uint32_t row = first + q * groups + group;
             const double v = group_sum(static_cast<double>(acc[q]) - static_cast<double>(comp[q]), log2g);
-            if (lig == 0 && row < ph.row_end)
-                pr_finish_row(row, v, re[q] - rs[q], rank_in, rank_out, contrib_out, outdeg, tele, base, damp, spread, dangling, my_diff,
-                              my_dangle);
+            if (lig == 0 && row < ph.row_end) {
+                double d = 0.0, g = 0.0;
+                pr_finish_row(row, v, re[q] - rs[q], rank_in, rank_out, contrib_out, outdeg, tele, base, damp,
+                              spread, dangling, d, g);
+                my_diff += to_fixed(d);
+                my_dangle += to_fixed(g);
+            }
         }
     } else {
         // Rows without entries: the teleport and dangling share only.
         const uint32_t row = ph.row_begin + (b - ph.first_block) * kPrThreads + threadIdx.x;
-        if (row < ph.row_end)
-            pr_finish_row(row, 0.0, 0, rank_in, rank_out, contrib_out, outdeg, tele, base, damp, spread, dangling, my_diff, my_dangle);
+        if (row < ph.row_end) {
+            double d = 0.0, g = 0.0;
+            pr_finish_row(row, 0.0, 0, rank_in, rank_out, contrib_out, outdeg, tele, base, damp, spread, dangling,
+                          d, g);
+            my_diff += to_fixed(d);
+            my_dangle += to_fixed(g);
+        }
     }
     }
-    my_diff = block_sum(my_diff, scratch);
-    my_dangle = block_sum(my_dangle, scratch);
+    }
+    unsigned long long* qscratch = reinterpret_cast<unsigned long long*>(scratch);
+    my_diff = block_sum(my_diff, qscratch);
+    my_dangle = block_sum(my_dangle, qscratch);
     if (threadIdx.x == 0) {
         row_partials[2 * blockIdx.x] = my_diff;
         row_partials[2 * blockIdx.x + 1] = my_dangle;
@@ -414,19 +455,22 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(
     const double* __restrict__ seg_partial, const float* __restrict__ rank_in, float* __restrict__ rank_out,
     float* __restrict__ contrib_out, const uint32_t* __restrict__ outdeg, const float* __restrict__ tele, uint32_t V,
     double base, double damp, PrState* __restrict__ state,
-    double tolerance, const double* __restrict__ row_partials, uint32_t row_blocks,
-    double* __restrict__ fin_partials) {
+    double tolerance, const unsigned long long* __restrict__ row_partials, uint32_t row_blocks,
+    unsigned long long* __restrict__ fin_partials, uint32_t* __restrict__ next_chunk) {
     if (state->done) return;
-    __shared__ double scratch[32];
+    __shared__ unsigned long long scratch[32];
     __shared__ bool s_last;
     const double dangling = state->dangling;
     const double spread = dangling / static_cast<double>(V);
-    double d = 0.0, g = 0.0;
+    unsigned long long d = 0, g = 0;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < long_rows) {
-        double sum = 0.0;
+        double sum = 0.0, rd = 0.0, rg = 0.0;
         for (uint32_t u = unit_begin[i]; u < unit_begin[i + 1]; ++u) sum += seg_partial[u];
-        pr_finish_row(i, sum, poff[i + 1] - poff[i], rank_in, rank_out, contrib_out, outdeg, tele, base, damp, spread, dangling, d, g);
+        pr_finish_row(i, sum, poff[i + 1] - poff[i], rank_in, rank_out, contrib_out, outdeg, tele, base, damp,
+                      spread, dangling, rd, rg);
+        d = to_fixed(rd);
+        g = to_fixed(rg);
     }
     const uint64_t slice_end = std::min<uint64_t>(static_cast<uint64_t>(blockIdx.x + 1) * kFinSlice, row_blocks);
     for (uint64_t k = static_cast<uint64_t>(blockIdx.x) * kFinSlice + threadIdx.x; k < slice_end; k += blockDim.x) {
@@ -445,7 +489,7 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    double dd = 0.0, gg = 0.0;
+    unsigned long long dd = 0, gg = 0;
     for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
         dd += __ldcg(fin_partials + 2 * k);
         gg += __ldcg(fin_partials + 2 * k + 1);
@@ -453,11 +497,13 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(
     dd = block_sum(dd, scratch);
     gg = block_sum(gg, scratch);
     if (threadIdx.x == 0) {
+        const double diff = from_fixed(dd);
         state->iterations += 1;
-        state->last_diff = dd;
-        state->dangling = gg;
-        if (dd < tolerance) state->done = 1;
+        state->last_diff = diff;
+        state->dangling = from_fixed(gg);
+        if (diff < tolerance) state->done = 1;
         state->ticket = 0;
+        *next_chunk = 0;  // the next iteration's row kernel starts its handout again
     }
 }
 
@@ -574,6 +620,60 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
     add(kPhaseEmpty, begin[0], end[0], 0, 0, static_cast<uint32_t>(ceil_div_u64(p.empty_rows, kPrThreads)));
     s.total_blocks = blocks;
     p.row_ctas = std::max<uint32_t>(1, std::min<uint32_t>(blocks, static_cast<uint32_t>(dev.sm_count) * kRowCtasPerSm));
+
+    // 5. Dispatch chunks: consecutive blocks grouped until their estimated work
+    // (entries plus a fixed cost per block) reaches kChunkWork, then ordered
+    // heaviest first so that the long poles start early.
+    {
+        constexpr uint64_t kBlockCost = 256, kChunkWork = 8192;
+        std::vector<uint32_t> hoff(static_cast<size_t>(V) + 1);
+        GCU_CUDA(cudaMemcpyAsync(hoff.data(), p.poff.ptr, sizeof(uint32_t) * hoff.size(), cudaMemcpyDeviceToHost,
+                                 dev.stream),
+                 "copy");
+        GCU_TRY(dev.sync());
+        auto block_work = [&](uint32_t b) -> uint64_t {
+            uint32_t pi = 0;
+            while (pi + 1 < s.nphases && s.phase[pi + 1].first_block <= b) ++pi;
+            const PrPhase& ph = s.phase[pi];
+            uint64_t entries = 0;
+            if (ph.kind == kPhaseLong) {
+                const uint2 u = units[b - ph.first_block];
+                const uint32_t deg = hoff[u.x + 1] - hoff[u.x];
+                entries = std::min<uint64_t>(kSegment, deg - u.y * kSegment);
+            } else if (ph.kind == kPhaseGroup) {
+                const uint64_t per_block = (kPrThreads >> ph.log2g) * static_cast<uint64_t>(kRowsPerGroup);
+                const uint64_t lo = ph.row_begin + (b - ph.first_block) * per_block;
+                const uint64_t hi = std::min<uint64_t>(lo + per_block, ph.row_end);
+                entries = hoff[hi] - hoff[lo];
+            }
+            return entries + kBlockCost;
+        };
+        std::vector<std::pair<uint64_t, uint2>> list;
+        uint32_t first = 0;
+        uint64_t work = 0;
+        for (uint32_t b = 0; b < blocks; ++b) {
+            work += block_work(b);
+            if (work >= kChunkWork || b + 1 == blocks) {
+                list.push_back({work, make_uint2(first, b + 1)});
+                first = b + 1;
+                work = 0;
+            }
+        }
+        std::stable_sort(list.begin(), list.end(),
+                         [](const std::pair<uint64_t, uint2>& x, const std::pair<uint64_t, uint2>& y) {
+                             return x.first > y.first;
+                         });
+        std::vector<uint2> chunks(list.size());
+        for (size_t i = 0; i < list.size(); ++i) chunks[i] = list[i].second;
+        p.nchunks = static_cast<uint32_t>(chunks.size());
+        GCU_TRY(p.chunks.allocate(dev, std::max<size_t>(chunks.size(), 1)));
+        GCU_TRY(p.next_chunk.allocate(dev, 1));
+        if (!chunks.empty())
+            GCU_CUDA(cudaMemcpyAsync(p.chunks.ptr, chunks.data(), sizeof(uint2) * chunks.size(),
+                                     cudaMemcpyHostToDevice, dev.stream),
+                     "copy");
+        GCU_TRY(dev.sync());  // the host vectors above go out of scope
+    }
     p.fin_blocks = static_cast<uint32_t>(
         std::max<uint64_t>({1, ceil_div_u64(p.long_rows, 256), ceil_div_u64(p.row_ctas, kFinSlice)}));
 
@@ -643,6 +743,7 @@ Error pagerank_ex(GraphImpl& g, bool directed, const float* tele_host, float dam
     init.last_diff = INFINITY;
     *p.host_state = init;
     GCU_CUDA(cudaMemcpyAsync(p.state.ptr, p.host_state, sizeof(PrState), cudaMemcpyHostToDevice, dev.stream), "copy");
+    GCU_CUDA(cudaMemsetAsync(p.next_chunk.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
 
     const double damp = static_cast<double>(damping);
     const double base = (1.0 - damp) / static_cast<double>(V);
@@ -664,10 +765,12 @@ Error pagerank_ex(GraphImpl& g, bool directed, const float* tele_host, float dam
             err = [&]() -> Error {
                 GCU_LAUNCH(dev, "pr_rows", pr_rows_kernel, p.row_ctas, kPrThreads, 0, p.poff.ptr, p.ptgt.ptr,
                            ranks[in], contrib[in], ranks[out], contrib[out], outdeg, d_tele, V, base, damp,
-                           p.state.ptr, p.sched, p.units.ptr, p.seg_partial.ptr, p.row_partials.ptr);
+                           p.state.ptr, p.sched, p.units.ptr, p.seg_partial.ptr, p.row_partials.ptr,
+                           p.chunks.ptr, p.nchunks, p.next_chunk.ptr);
                 GCU_LAUNCH(dev, "pr_finish", pr_finish_kernel, p.fin_blocks, 256, 0, p.poff.ptr, p.long_rows,
                            p.unit_begin.ptr, p.seg_partial.ptr, ranks[in], ranks[out], contrib[out], outdeg, d_tele,
-                           V, base, damp, p.state.ptr, tol, p.row_partials.ptr, p.row_ctas, p.fin_partials.ptr);
+                           V, base, damp, p.state.ptr, tol, p.row_partials.ptr, p.row_ctas, p.fin_partials.ptr,
+                           p.next_chunk.ptr);
                 return ok();
             }();
         }

@@ -95,7 +95,7 @@ def test_batch_errors(device):
         G.GpuBatch.from_csr([0, 2, 3], [0, 1, 2, 3], [1, 2, 1], device)
     assert "leaves its graph" in str(e.value)
     with pytest.raises(GrafeoCudaError) as e:
-        G.GpuBatch.from_csr([0, 2, 3], [0, 1, 1], [2, 0], device)  # invalid CSR first
+        G.GpuBatch.from_csr([0, 1, 2], [0, 2, 1], [1], device)  # offsets decrease: invalid CSR first
     assert e.value.status == G.ERR_INVALID_CSR
     b = G.GpuBatch.from_graphs([([0, 1, 2], [1, 0]), ([0, 0], [])], device)
     with pytest.raises(GrafeoCudaError):
