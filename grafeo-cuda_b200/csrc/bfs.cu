@@ -14,7 +14,9 @@
 //  * Bottom-up step (large frontiers, symmetric graphs only): every unvisited
 //    vertex scans its list for a parent in the frontier bitmap and stops at the
 //    first hit (Beamer, Asanovic and Patterson, SC'12). No atomics: each warp
-//    owns one bitmap word of 32 vertices.
+//    owns one bitmap word of 32 vertices; a lane checks the first entries of
+//    its vertex's list alone and longer lists are walked by the whole warp,
+//    32 coalesced entries per step.
 //  * Three step variants: push with one warp per frontier vertex (one
 //    launch), load-balanced push (above), pull (above).
 //  * Schedule: Beamer's alpha/beta rule (alpha = 14, beta = 24) over the
@@ -86,23 +88,38 @@ __device__ __forceinline__ void append_warp(bool take, uint32_t v, uint32_t* __r
     if (take) queue[base + __popc(mask & ((1u << lane) - 1))] = v;
 }
 
+// Per-lane totals of what a lane labelled; a warp adds them to the level's
+// counters once, when it is done (flush_tally), instead of one atomic pair on
+// the same two words per warp step.
+struct Tally {
+    uint32_t found = 0;
+    unsigned long long edges = 0;
+};
+
 // Labels v (found by a parent at this level) and records it; called by all
 // lanes of a warp, `found` says whether this lane discovered a vertex.
 __device__ __forceinline__ void record_discovery(bool found, uint32_t v, const uint32_t* __restrict__ offsets,
                                                  int32_t* __restrict__ dist, int32_t level,
-                                                 uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr) {
+                                                 uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr,
+                                                 Tally& tally) {
     uint32_t deg = 0;
     if (found) {
         dist[v] = level;
         deg = offsets[v + 1] - offsets[v];
+        tally.found += 1;
+        tally.edges += deg;
     }
-    const unsigned found_mask = __ballot_sync(kFullMask, found);
-    if (found_mask == 0) return;
-    unsigned long long e = warp_sum(static_cast<unsigned long long>(deg));
+    if (__ballot_sync(kFullMask, found) == 0) return;
     append_warp(found && deg > 0, v, next_queue, &ctr->queued);
-    if (lane_id() == static_cast<unsigned>(__ffs(found_mask) - 1)) {
-        atomicAdd(&ctr->discovered, static_cast<uint32_t>(__popc(found_mask)));
-        if (e) atomicAdd(&ctr->edges, e);
+}
+
+// All 32 lanes call it once, at the end of the kernel.
+__device__ __forceinline__ void flush_tally(const Tally& tally, BfsCounters* __restrict__ ctr) {
+    const uint32_t found = warp_sum(tally.found);
+    const unsigned long long edges = warp_sum(tally.edges);
+    if (lane_id() == 0) {
+        if (found) atomicAdd(&ctr->discovered, found);
+        if (edges) atomicAdd(&ctr->edges, edges);
     }
 }
 
@@ -161,6 +178,7 @@ __global__ void __launch_bounds__(kTdThreads) bfs_topdown_kernel(
         s_start[k] = offsets[queue[i0 + k]];
     }
     __syncthreads();
+    Tally tally;
 #pragma unroll
     for (int q = 0; q < kTdItems; ++q) {
         const uint32_t e = static_cast<uint32_t>(e0) + q * kTdThreads + threadIdx.x;
@@ -179,8 +197,9 @@ __global__ void __launch_bounds__(kTdThreads) bfs_topdown_kernel(
             const uint32_t bit = 1u << (v & 31);
             if (!(__ldcg(visited + (v >> 5)) & bit)) found = !(atomicOr(visited + (v >> 5), bit) & bit);
         }
-        record_discovery(found, v, offsets, dist, next_level, next_queue, ctr);
+        record_discovery(found, v, offsets, dist, next_level, next_queue, ctr, tally);
     }
+    flush_tally(tally, ctr);
 }
 
 __global__ void bfs_queue_to_bitmap_kernel(const uint32_t* __restrict__ queue, uint32_t n,
@@ -192,7 +211,19 @@ __global__ void bfs_queue_to_bitmap_kernel(const uint32_t* __restrict__ queue, u
     }
 }
 
-// Bottom-up: warp w handles the 32 vertices of bitmap word w.
+constexpr uint32_t kBuSolo = 8;  // entries a lane checks alone before its warp takes over the list
+
+__device__ __forceinline__ bool in_frontier(const uint32_t* __restrict__ frontier, uint32_t u) {
+    return (__ldg(frontier + (u >> 5)) >> (u & 31)) & 1u;
+}
+
+// Bottom-up: warp w handles the 32 vertices of bitmap word w. Each unvisited
+// vertex first checks its first kBuSolo entries alone (4 loads in flight);
+// most vertices that have a parent in a large frontier find it there. The
+// lists that are left are then walked by the whole warp, one list at a time,
+// 32 consecutive entries per step (coalesced) with a ballot to stop at the
+// first parent, so a long list neither serialises one lane nor stalls the
+// other 31.
 __global__ void __launch_bounds__(kBuThreads) bfs_bottomup_kernel(
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t V,
     const uint32_t* __restrict__ frontier, uint32_t* __restrict__ next_frontier, uint32_t* __restrict__ visited,
@@ -201,27 +232,49 @@ __global__ void __launch_bounds__(kBuThreads) bfs_bottomup_kernel(
     const unsigned lane = lane_id();
     const uint64_t words = ceil_div_u64(V, 32);
     const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    Tally tally;
     for (uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; w < words; w += warps) {
         const uint32_t vis = visited[w];
         const uint32_t v = static_cast<uint32_t>(w * 32 + lane);
         bool found = false;
+        uint32_t s = 0, e = 0;
         if (v < V && !((vis >> lane) & 1u)) {
-            const uint32_t end = offsets[v + 1];
-            for (uint32_t j = offsets[v]; j < end; ++j) {
-                const uint32_t u = targets[j];
-                if ((__ldg(frontier + (u >> 5)) >> (u & 31)) & 1u) {
-                    found = true;
+            s = offsets[v];
+            e = offsets[v + 1];
+        }
+        const uint32_t solo = min(e - s, kBuSolo);
+        for (uint32_t k = 0; k < solo && !found; k += 4) {
+            uint32_t t[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) t[q] = k + q < solo ? targets[s + k + q] : 0xFFFFFFFFu;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) found = found || (t[q] != 0xFFFFFFFFu && in_frontier(frontier, t[q]));
+        }
+        unsigned pending = __ballot_sync(kFullMask, !found && e - s > kBuSolo);
+        while (pending) {
+            const int p = __ffs(pending) - 1;
+            pending &= pending - 1;
+            const uint64_t ps = static_cast<uint64_t>(__shfl_sync(kFullMask, s, p)) + kBuSolo;
+            const uint64_t pe = __shfl_sync(kFullMask, e, p);
+            bool hit = false;
+            for (uint64_t base = ps; base < pe; base += 32) {
+                const uint64_t j = base + lane;
+                const bool h = j < pe && in_frontier(frontier, targets[j]);
+                if (__ballot_sync(kFullMask, h)) {
+                    hit = true;
                     break;
                 }
             }
+            if (static_cast<int>(lane) == p) found = hit;
         }
         const unsigned mask = __ballot_sync(kFullMask, found);
         if (lane == 0) {
             next_frontier[w] = mask;
             if (mask) visited[w] = vis | mask;
         }
-        record_discovery(found, v, offsets, dist, next_level, next_queue, ctr);
+        record_discovery(found, v, offsets, dist, next_level, next_queue, ctr, tally);
     }
+    flush_tally(tally, ctr);
 }
 
 // Top-down, one warp per frontier vertex (no degree scan: one launch, for
@@ -232,6 +285,7 @@ __global__ void __launch_bounds__(kTdThreads) bfs_topdown_warp_kernel(
     BfsCounters* __restrict__ ctr, int32_t next_level) {
     const unsigned lane = lane_id();
     const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    Tally tally;
     for (uint64_t i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < qsize; i += nwarps) {
         const uint32_t u = queue[i];
         const uint64_t s = offsets[u], e = offsets[u + 1];
@@ -244,9 +298,10 @@ __global__ void __launch_bounds__(kTdThreads) bfs_topdown_warp_kernel(
                 const uint32_t bit = 1u << (v & 31);
                 if (!(__ldcg(visited + (v >> 5)) & bit)) found = !(atomicOr(visited + (v >> 5), bit) & bit);
             }
-            record_discovery(found, v, offsets, dist, next_level, next_queue, ctr);
+            record_discovery(found, v, offsets, dist, next_level, next_queue, ctr, tally);
         }
     }
+    flush_tally(tally, ctr);
 }
 
 // One warp: the features of the decision before expanding the frontier the

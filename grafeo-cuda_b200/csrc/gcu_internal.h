@@ -159,6 +159,7 @@ struct DeviceBuffer {
 
 struct PageRankPlan;
 struct BfsWork;
+struct KtCache;
 
 // Per-graph degree statistics that the learned schedule's features use.
 struct DegreeStats {
@@ -179,6 +180,7 @@ struct GraphImpl {
     PageRankPlan* pr_plan = nullptr;  // owned; freed by destroy_pagerank_plan
     PageRankPlan* pr_plan_directed = nullptr;  // pull over the transpose; owned
     BfsWork* bfs_work = nullptr;      // owned; freed by destroy_bfs_work
+    KtCache* kt_cache = nullptr;      // owned; freed by destroy_kt_cache
     bool has_degree_stats = false;
     DegreeStats degree_stats;
     ~GraphImpl();
@@ -246,6 +248,7 @@ Error pagerank_ex(GraphImpl& g, bool directed, const float* tele, float damping,
 
 void destroy_pagerank_plan(PageRankPlan* p);
 void destroy_bfs_work(BfsWork* w);
+void destroy_kt_cache(KtCache* c);
 
 // ---------------------------------------------------------------- device CSR build
 

@@ -339,39 +339,80 @@ static Error triangle_support(GraphImpl& g, const uint32_t* rev, uint32_t* suppo
     return ok();
 }
 
-// Symmetric CSR: per-edge triangle counts from the DAG, then incremental
-// peeling. Every round removes exactly the entries the reference's round
-// removes, so the edge list and the round count are the same.
-static Error k_truss_symmetric(GraphImpl& g, uint32_t k, const uint32_t* src, const uint32_t* rev,
-                               std::vector<uint32_t>* edges, uint32_t* iterations) {
-    DeviceImpl& dev = *g.dev;
-    const uint32_t E = g.num_edges, V = g.num_nodes;
-    const uint32_t threshold = k - 2;
-    DeviceBuffer<uint32_t> support, state, removed, scratch;
+// Per-graph state of the symmetric k-truss: row of every entry, reverse
+// entries, self-loop flags and the triangle support of every u < v entry. It
+// depends only on the graph, so it is computed once and reused by every
+// k_truss call and by the truss decomposition (3 E + V words of HBM, kept
+// with the graph like the PageRank plan).
+struct KtCache {
+    DeviceBuffer<uint32_t> src, rev, support;
     DeviceBuffer<uint8_t> loop;
+    uint32_t loops = 0;  // self-loop entries
+};
+
+void destroy_kt_cache(KtCache* c) { delete c; }
+
+static Error ensure_kt_cache(GraphImpl& g, KtCache** out) {
+    if (!g.kt_cache) {
+        DeviceImpl& dev = *g.dev;
+        const uint32_t E = g.num_edges, V = g.num_nodes;
+        auto c = std::unique_ptr<KtCache, void (*)(KtCache*)>(new KtCache, destroy_kt_cache);
+        GCU_TRY(c->src.allocate(dev, E));
+        GCU_TRY(c->rev.allocate(dev, E));
+        GCU_TRY(c->support.allocate(dev, E));
+        GCU_TRY(c->loop.allocate(dev, V));
+        DeviceBuffer<uint32_t> count;
+        GCU_TRY(count.allocate(dev, 1));
+        const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+        const unsigned row_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
+        const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
+        GCU_LAUNCH(dev, "kt_rows", kt_rows_kernel, row_grid, 256, 0, g.offsets.ptr, V, c->src.ptr);
+        GCU_LAUNCH(dev, "kt_reverse", kt_reverse_kernel, edge_grid, 256, 0, g.offsets.ptr, g.targets.ptr, c->src.ptr,
+                   E, c->rev.ptr);
+        GCU_CUDA(cudaMemsetAsync(c->loop.ptr, 0, V, dev.stream), "memset");
+        GCU_CUDA(cudaMemsetAsync(count.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
+        GCU_LAUNCH(dev, "kt_loops", kt_loops_kernel, edge_grid, 256, 0, g.targets.ptr, c->src.ptr, E, c->loop.ptr,
+                   count.ptr);
+        GCU_CUDA(cudaMemsetAsync(c->support.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
+        GCU_TRY(triangle_support(g, c->rev.ptr, c->support.ptr));
+        GCU_CUDA(cudaMemcpyAsync(&c->loops, count.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+        GCU_TRY(dev.sync());
+        g.kt_cache = c.release();
+    }
+    *out = g.kt_cache;
+    return ok();
+}
+
+// Symmetric CSR: per-edge triangle counts from the DAG (cached), then
+// incremental peeling. Every round removes exactly the entries the
+// reference's round removes, so the edge list and the round count are the
+// same.
+static Error k_truss_symmetric(GraphImpl& g, uint32_t k, std::vector<uint32_t>* edges, uint32_t* iterations) {
+    DeviceImpl& dev = *g.dev;
+    const uint32_t E = g.num_edges;
+    const uint32_t threshold = k - 2;
+    KtCache* c = nullptr;
+    GCU_TRY(ensure_kt_cache(g, &c));
+    const uint32_t* src = c->src.ptr;
+    const uint32_t* rev = c->rev.ptr;
+    DeviceBuffer<uint32_t> support, state, removed, scratch;
     GCU_TRY(support.allocate(dev, static_cast<uint64_t>(E) + 1));
     GCU_TRY(state.allocate(dev, static_cast<uint64_t>(E) + 1));
     GCU_TRY(removed.allocate(dev, E));
-    GCU_TRY(loop.allocate(dev, V));
-    GCU_TRY(scratch.allocate(dev, 2));  // [0] removed this round, [1] self-loops
-    GCU_CUDA(cudaMemsetAsync(support.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
+    GCU_TRY(scratch.allocate(dev, 1));  // removed this round
+    GCU_CUDA(cudaMemcpyAsync(support.ptr, c->support.ptr, sizeof(uint32_t) * static_cast<size_t>(E),
+                             cudaMemcpyDeviceToDevice, dev.stream),
+             "copy");
     GCU_CUDA(cudaMemsetAsync(state.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
-    GCU_CUDA(cudaMemsetAsync(loop.ptr, 0, V, dev.stream), "memset");
-    GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, 2 * sizeof(uint32_t), dev.stream), "memset");
     const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
     const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
-    GCU_LAUNCH(dev, "kt_loops", kt_loops_kernel, edge_grid, 256, 0, g.targets.ptr, src, E, loop.ptr, scratch.ptr + 1);
-
-    GCU_TRY(triangle_support(g, rev, support.ptr));
-    uint32_t loops = 0;
-    GCU_CUDA(cudaMemcpyAsync(&loops, scratch.ptr + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
-    GCU_TRY(dev.sync());
+    const uint32_t loops = c->loops;
 
     uint32_t round = 1;
     while (true) {
         GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
-        GCU_LAUNCH(dev, "kt_round_filter", kt_round_filter_kernel, edge_grid, 256, 0, g.targets.ptr, src, loop.ptr,
-                   support.ptr, state.ptr, E, threshold, round, removed.ptr, scratch.ptr, nullptr, 0u);
+        GCU_LAUNCH(dev, "kt_round_filter", kt_round_filter_kernel, edge_grid, 256, 0, g.targets.ptr, src,
+                   c->loop.ptr, support.ptr, state.ptr, E, threshold, round, removed.ptr, scratch.ptr, nullptr, 0u);
         uint32_t n = 0;
         GCU_CUDA(cudaMemcpyAsync(&n, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
         GCU_TRY(dev.sync());
@@ -400,6 +441,7 @@ Error k_truss(GraphImpl& g, uint32_t k, std::vector<uint32_t>* edges, uint32_t* 
     DeviceImpl& dev = *g.dev;
     bool symmetric = false;
     GCU_TRY(graph_symmetry(g, &symmetric));
+    if (symmetric) return k_truss_symmetric(g, k, edges, iterations);
     DeviceBuffer<uint32_t> src, rev;
     GCU_TRY(src.allocate(dev, E));
     GCU_TRY(rev.allocate(dev, E));
@@ -409,11 +451,66 @@ Error k_truss(GraphImpl& g, uint32_t k, std::vector<uint32_t>* edges, uint32_t* 
     GCU_LAUNCH(dev, "kt_rows", kt_rows_kernel, row_grid, 256, 0, g.offsets.ptr, V, src.ptr);
     GCU_LAUNCH(dev, "kt_reverse", kt_reverse_kernel, edge_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src.ptr, E,
                rev.ptr);
-    if (symmetric) return k_truss_symmetric(g, k, src.ptr, rev.ptr, edges, iterations);
     return k_truss_general(g, k, src.ptr, rev.ptr, edges, iterations);
 }
 
 // ---------------------------------------------------------------- truss decomposition
+
+// Appends, warp-aggregated, the entries with take set (all 32 lanes call it).
+__device__ __forceinline__ void kt_append(bool take, uint32_t j, uint32_t* __restrict__ list,
+                                          uint32_t* __restrict__ count) {
+    const unsigned mask = __ballot_sync(kFullMask, take);
+    if (mask == 0) return;
+    const unsigned lane = lane_id();
+    const int leader = __ffs(mask) - 1;
+    uint32_t at = 0;
+    if (lane == static_cast<unsigned>(leader)) at = atomicAdd(count, static_cast<uint32_t>(__popc(mask)));
+    at = __shfl_sync(kFullMask, at, leader);
+    if (take) list[at + __popc(mask & ((1u << lane) - 1))] = j;
+}
+
+// The alive u < v entries: from all E entries (list == nullptr) or from a
+// previous active list of n entries.
+__global__ void kt_active_kernel(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ src,
+                                 const uint32_t* __restrict__ state, const uint32_t* __restrict__ list, uint32_t n,
+                                 uint32_t* __restrict__ out, uint32_t* __restrict__ count) {
+    for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~31ull; base < n;
+         base += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t i = base + lane_id();
+        bool take = false;
+        uint32_t j = 0;
+        if (i < n) {
+            j = list ? list[i] : static_cast<uint32_t>(i);
+            take = state[j] == 0 && targets[j] > src[j];
+        }
+        kt_append(take, j, out, count);
+    }
+}
+
+// kt_round_filter_kernel over an active list: every listed entry still alive
+// with support < threshold is removed in this round (state = round), listed in
+// `removed` and given truss_value.
+__global__ void kt_active_filter_kernel(const uint32_t* __restrict__ active, uint32_t n,
+                                        const uint32_t* __restrict__ support, uint32_t* __restrict__ state,
+                                        uint32_t threshold, uint32_t round, uint32_t* __restrict__ removed,
+                                        uint32_t* __restrict__ removed_count, uint32_t* __restrict__ truss,
+                                        uint32_t truss_value) {
+    for (uint64_t base = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) & ~31ull; base < n;
+         base += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t i = base + lane_id();
+        bool take = false;
+        uint32_t j = 0;
+        if (i < n) {
+            j = active[i];
+            take = state[j] == 0 && support[j] < threshold;
+            if (take) {
+                state[j] = round;
+                truss[j] = truss_value;
+            }
+        }
+        kt_append(take, j, removed, removed_count);
+    }
+}
 
 // Spreads the u < v entries' trussness to every entry: the reverse entry gets
 // the same value, self-loops 0.
@@ -435,49 +532,51 @@ __global__ void kt_truss_spread_kernel(const uint32_t* __restrict__ targets, con
 Error truss_decomposition(GraphImpl& g, uint32_t* host_truss, uint32_t* max_truss, uint32_t* rounds) {
     *max_truss = 0;
     *rounds = 0;
-    const uint32_t E = g.num_edges, V = g.num_nodes;
+    const uint32_t E = g.num_edges;
     if (E == 0) return ok();
     DeviceImpl& dev = *g.dev;
     bool symmetric = false;
     GCU_TRY(graph_symmetry(g, &symmetric));
     if (!symmetric) return kernel_error("truss decomposition needs a symmetric CSR (every u -> v with its v -> u)");
-    DeviceBuffer<uint32_t> src, rev, support, state, removed, truss, scratch;
-    GCU_TRY(src.allocate(dev, E));
-    GCU_TRY(rev.allocate(dev, E));
+    KtCache* c = nullptr;
+    GCU_TRY(ensure_kt_cache(g, &c));
+    const uint32_t* src = c->src.ptr;
+    const uint32_t* rev = c->rev.ptr;
+    DeviceBuffer<uint32_t> support, state, removed, truss, scratch, active[2];
     GCU_TRY(support.allocate(dev, E));
     GCU_TRY(state.allocate(dev, E));
     GCU_TRY(removed.allocate(dev, E));
     GCU_TRY(truss.allocate(dev, E));
-    GCU_TRY(scratch.allocate(dev, 2));
+    GCU_TRY(scratch.allocate(dev, 2));  // [0] removed this round, [1] active count
     const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
-    const unsigned row_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
     const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
-    GCU_LAUNCH(dev, "kt_rows", kt_rows_kernel, row_grid, 256, 0, g.offsets.ptr, V, src.ptr);
-    GCU_LAUNCH(dev, "kt_reverse", kt_reverse_kernel, edge_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src.ptr, E,
-               rev.ptr);
-    GCU_CUDA(cudaMemsetAsync(support.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
+    GCU_CUDA(cudaMemcpyAsync(support.ptr, c->support.ptr, sizeof(uint32_t) * static_cast<size_t>(E),
+                             cudaMemcpyDeviceToDevice, dev.stream),
+             "copy");
     GCU_CUDA(cudaMemsetAsync(state.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
     GCU_CUDA(cudaMemsetAsync(truss.ptr, 0, sizeof(uint32_t) * static_cast<size_t>(E), dev.stream), "memset");
-    GCU_TRY(triangle_support(g, rev.ptr, support.ptr));
     // Undirected edges alive: in a symmetric CSR every edge but a self-loop
-    // has two entries, so there are (E - self-loop entries) / 2 of them.
-    DeviceBuffer<uint8_t> loop;
-    GCU_TRY(loop.allocate(dev, V));
-    GCU_CUDA(cudaMemsetAsync(loop.ptr, 0, V, dev.stream), "memset");
-    GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, 2 * sizeof(uint32_t), dev.stream), "memset");
-    GCU_LAUNCH(dev, "kt_loops", kt_loops_kernel, edge_grid, 256, 0, g.targets.ptr, src.ptr, E, loop.ptr,
-               scratch.ptr + 1);
-    uint32_t loops = 0;
-    GCU_CUDA(cudaMemcpyAsync(&loops, scratch.ptr + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
-    GCU_TRY(dev.sync());
-    uint64_t alive = (static_cast<uint64_t>(E) - loops) / 2;
+    // has two entries, so there are (E - self-loop entries) / 2 of them; the
+    // active list holds their u < v entries and is compacted whenever half
+    // of it has been peeled, so late rounds only touch the remaining core.
+    uint64_t alive = (static_cast<uint64_t>(E) - c->loops) / 2;
+    const uint64_t list_cap = std::max<uint64_t>(alive, 1);
+    GCU_TRY(active[0].allocate(dev, list_cap));
+    GCU_TRY(active[1].allocate(dev, list_cap));
+    GCU_CUDA(cudaMemsetAsync(scratch.ptr + 1, 0, sizeof(uint32_t), dev.stream), "memset");
+    GCU_LAUNCH(dev, "kt_active", kt_active_kernel, edge_grid, 256, 0, g.targets.ptr, src, state.ptr,
+               static_cast<const uint32_t*>(nullptr), E, active[0].ptr, scratch.ptr + 1);
+    int cur = 0;
+    uint64_t listed = alive;  // entries in active[cur]
     uint32_t round = 0, k = 3, top = alive > 0 ? 2 : 0;
     while (alive > 0) {
         round += 1;
+        const unsigned grid =
+            static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(listed, 256), cap)));
         GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
-        GCU_LAUNCH(dev, "kt_round_filter", kt_round_filter_kernel, edge_grid, 256, 0, g.targets.ptr, src.ptr,
-                   static_cast<const uint8_t*>(nullptr), support.ptr, state.ptr, E, k - 2, round, removed.ptr,
-                   scratch.ptr, truss.ptr, k - 1);
+        GCU_LAUNCH(dev, "kt_active_filter", kt_active_filter_kernel, grid, 256, 0, active[cur].ptr,
+                   static_cast<uint32_t>(listed), support.ptr, state.ptr, k - 2, round, removed.ptr, scratch.ptr,
+                   truss.ptr, k - 1);
         uint32_t n = 0;
         GCU_CUDA(cudaMemcpyAsync(&n, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
         GCU_TRY(dev.sync());
@@ -490,13 +589,20 @@ Error truss_decomposition(GraphImpl& g, uint32_t* host_truss, uint32_t* max_trus
         alive -= n;
         const unsigned peel_grid =
             static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(static_cast<uint64_t>(n) * 32, 256), cap));
-        GCU_LAUNCH(dev, "kt_peel", kt_peel_kernel, peel_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src.ptr, rev.ptr,
+        GCU_LAUNCH(dev, "kt_peel", kt_peel_kernel, peel_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src, rev,
                    state.ptr, support.ptr, removed.ptr, scratch.ptr, round);
+        if (alive > 0 && 2 * alive < listed) {
+            GCU_CUDA(cudaMemsetAsync(scratch.ptr + 1, 0, sizeof(uint32_t), dev.stream), "memset");
+            GCU_LAUNCH(dev, "kt_active", kt_active_kernel, grid, 256, 0, g.targets.ptr, src, state.ptr,
+                       active[cur].ptr, static_cast<uint32_t>(listed), active[cur ^ 1].ptr, scratch.ptr + 1);
+            cur ^= 1;
+            listed = alive;
+        }
     }
     *max_truss = top;
     *rounds = round;
     if (host_truss) {
-        GCU_LAUNCH(dev, "kt_truss_spread", kt_truss_spread_kernel, edge_grid, 256, 0, g.targets.ptr, src.ptr, rev.ptr,
+        GCU_LAUNCH(dev, "kt_truss_spread", kt_truss_spread_kernel, edge_grid, 256, 0, g.targets.ptr, src, rev,
                    truss.ptr, E, support.ptr);
         GCU_CUDA(cudaMemcpyAsync(host_truss, support.ptr, sizeof(uint32_t) * static_cast<size_t>(E),
                                  cudaMemcpyDeviceToHost, dev.stream),

@@ -21,20 +21,21 @@
 //    4 steps per trip, so every lane keeps 8 independent loads in flight within
 //    32 registers (8 CTAs per SM, persistent); consecutive groups read
 //    consecutive rows (coalesced), and there is no search, staging, barrier or
-//    carry. Rows of 4096 or more entries are split into 4096-entry segments,
-//    one block each, and their partial sums are added in segment order by the
+//    carry. Rows of 1024 or more entries are split into 1024-entry segments,
+//    one warp each, and their partial sums are added in segment order by the
 //    finishing kernel.
-//  * Work blocks (a long-row segment, or 2 rows per lane group of one class)
-//    are grouped into chunks of about equal estimated work, ordered heaviest
-//    first, and the persistent CTAs take chunks from a counter, so a CTA that
-//    drew heavy rows takes fewer.
+//  * Work units (a long-row segment, one warp's rows of a class, or 32 rows
+//    without entries) are dealt round-robin to the warps of the persistent
+//    grid: every class is spread evenly, the warps in flight read one
+//    contiguous window of the CSR, and no block barrier ties the warps of a
+//    CTA together.
 //  * Row sums: FP32 Kahan sums per lane, FP64 across lanes (shuffle tree) and
 //    across segments. Epilogue per row v: r'[v] = (1-d)/N + d (sum +
 //    dangling/N); |r' - r| and the dangling mass of r' are summed as 64-bit
 //    fixed-point integers (2^-62 units) per CTA and reduced by the last block
 //    of the finishing kernel: integer sums do not depend on the order, so the
-//    result is deterministic whichever CTA took which chunk (no float
-//    atomics); c'[v] = r'[v] / deg(v) is written for the next iteration.
+//    result is deterministic whatever the grid size (no float atomics);
+//    c'[v] = r'[v] / deg(v) is written for the next iteration.
 //  * The iteration loop stays on the device: each kernel reads a `done` flag
 //    first, so the host queues iterations ahead and polls the flag once per
 //    chunk instead of syncing every iteration.
@@ -49,8 +50,8 @@ namespace gcu {
 
 constexpr int kPrThreads = 256;
 constexpr int kDegClasses = 33;       // class 0: degree 0; class c: degree in [2^(c-1), 2^c)
-constexpr int kLongClass = 13;        // degree >= 4096
-constexpr uint32_t kSegment = 4096;   // entries per long-row segment (one block)
+constexpr int kLongClass = 11;        // degree >= 1024
+constexpr uint32_t kSegment = 1024;   // entries per long-row segment (one warp)
 constexpr int kClassBlock = 1024;     // vertices per block of the class partition
 constexpr int kMaxPhases = 16;
 constexpr int kRowsPerGroup = 2;      // rows a lane group works on in lockstep
@@ -60,7 +61,7 @@ constexpr int kRowCtasPerSm = 8;      // persistent CTAs of the row kernel per S
 enum : uint32_t { kPhaseLong = 0, kPhaseGroup = 1, kPhaseEmpty = 2 };
 
 struct PrPhase {
-    uint32_t first_block;  // first block of this phase
+    uint32_t first_block;  // first work unit of this phase
     uint32_t row_begin, row_end;
     uint32_t kind;
     uint32_t log2g;        // lanes per row = 1 << log2g (group phases)
@@ -83,7 +84,7 @@ struct PrState {
 };
 
 struct PageRankPlan {
-    uint32_t long_rows = 0;   // rows [0, long_rows) of the relabelled CSR have >= 4096 entries
+    uint32_t long_rows = 0;   // rows [0, long_rows) of the relabelled CSR have >= 1024 entries
     uint32_t empty_rows = 0;  // rows without entries (the last class)
     uint32_t dangling_rows = 0;  // vertices without out-edges
     uint32_t fin_blocks = 1;
@@ -102,9 +103,6 @@ struct PageRankPlan {
     DeviceBuffer<float> ranks_out;     // V: result in original order
     DeviceBuffer<unsigned long long> row_partials; // 2 fixed-point sums per CTA of the row kernel
     DeviceBuffer<unsigned long long> fin_partials; // 2 per block of the finishing kernel
-    DeviceBuffer<uint2> chunks;        // [first, end) block ranges, heaviest first
-    uint32_t nchunks = 0;
-    DeviceBuffer<uint32_t> next_chunk; // dispatch counter of the row kernel (reset by the finishing kernel)
     DeviceBuffer<PrState> state;
     PrState* host_state = nullptr;     // pinned
 };
@@ -313,134 +311,141 @@ __device__ __forceinline__ double group_sum(double v, uint32_t log2g) {
     return v;
 }
 
-// Persistent: each CTA takes chunks of consecutive work blocks from a counter
-// (chunks of about equal estimated work, the heaviest first), so a CTA that
-// drew heavy rows takes fewer chunks. 8 CTAs of 256 threads per SM.
+// Persistent: warp w of W works on units w, w + W, w + 2W, ... (a unit is a
+// 1024-entry segment of a long row, the 2 rows per lane group of one warp in a
+// degree class, or 32 rows without entries). Every phase's units are spread
+// evenly over the warps, the warps in flight read one contiguous window of
+// the CSR, and no block barrier ties the warps of a CTA together inside the
+// loop. 8 CTAs of 256 threads per SM.
 __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
     const uint32_t* __restrict__ poff, const uint32_t* __restrict__ ptgt, const float* __restrict__ rank_in,
     const float* __restrict__ contrib_in, float* __restrict__ rank_out, float* __restrict__ contrib_out,
     const uint32_t* __restrict__ outdeg, const float* __restrict__ tele, uint32_t V, double base, double damp,
     const PrState* __restrict__ state, const PrSchedule sched,
     const uint2* __restrict__ units, double* __restrict__ seg_partial,
-    unsigned long long* __restrict__ row_partials, const uint2* __restrict__ chunks, uint32_t nchunks,
-    uint32_t* __restrict__ next_chunk) {
+    unsigned long long* __restrict__ row_partials) {
     if (state->done) return;
-    __shared__ double scratch[32];
-    __shared__ uint32_t s_chunk[2];
-    const double dangling = state->dangling;
-    const double spread = dangling / static_cast<double>(V);
-    unsigned long long my_diff = 0, my_dangle = 0;
-    for (uint32_t trip = 0;; ++trip) {
-    // Two slots: a slot is rewritten two trips later, after every thread has
-    // passed the barrier of the trip in between.
-    if (threadIdx.x == 0) s_chunk[trip & 1] = atomicAdd(next_chunk, 1u);
-    __syncthreads();
-    const uint32_t ci = s_chunk[trip & 1];
-    if (ci >= nchunks) break;
-    const uint2 chunk = chunks[ci];
-    for (uint32_t b = chunk.x; b < chunk.y; ++b) {
-    uint32_t pi = 0;
-    while (pi + 1 < sched.nphases && sched.phase[pi + 1].first_block <= b) ++pi;
-    const PrPhase ph = sched.phase[pi];
-
-    if (ph.kind == kPhaseLong) {
-        // One segment of a long row: 16 entries per thread, 4 loads in flight.
-        const uint2 unit = units[b - ph.first_block];
-        const uint32_t row_start = poff[unit.x], row_end = poff[unit.x + 1];
-        const uint32_t s0 = row_start + unit.y * kSegment;
-        const uint32_t s1 = min(s0 + kSegment, row_end);
-        float acc = 0.f, comp = 0.f;
-        uint32_t j = s0 + threadIdx.x;
-        for (; j + 7 * kPrThreads < s1; j += 8 * kPrThreads) {
-            uint32_t t[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) t[q] = ld_stream(ptgt + j + q * kPrThreads);
-            float c[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) c[q] = __ldg(contrib_in + t[q]);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) kahan_add(acc, comp, c[q]);
-        }
-        for (; j < s1; j += kPrThreads) kahan_add(acc, comp, __ldg(contrib_in + ld_stream(ptgt + j)));
-        const double part = block_sum(static_cast<double>(acc) - static_cast<double>(comp), scratch);
-        if (threadIdx.x == 0) seg_partial[b - ph.first_block] = part;
-    } else if (ph.kind == kPhaseGroup) {
-        // Rows of one class, 2^log2g lanes per row, kRowsPerGroup rows per
-        // group worked on in lockstep: each step issues one target load and
-        // one gather per row (8 in flight per lane with the kUnroll-step
-        // unroll), so no row waits on the previous one's memory round trips.
-        const uint32_t log2g = ph.log2g, g = 1u << log2g;
-        const uint32_t groups = kPrThreads >> log2g;
-        const uint32_t group = threadIdx.x >> log2g, lig = threadIdx.x & (g - 1);
-        const uint32_t first = ph.row_begin + (b - ph.first_block) * groups * kRowsPerGroup;
-        uint32_t rs[kRowsPerGroup], re[kRowsPerGroup];
-        uint32_t longest = 0;
-#pragma unroll
-        for (int q = 0; q < kRowsPerGroup; ++q) {
-            const uint32_t row = first + q * groups + group;
-            rs[q] = 0;
-            re[q] = 0;
-            if (row < ph.row_end) {
-                rs[q] = poff[row];
-                re[q] = poff[row + 1];
-            }
-            longest = max(longest, re[q] - rs[q]);
-        }
-        float acc[kRowsPerGroup], comp[kRowsPerGroup];
-#pragma unroll
-        for (int q = 0; q < kRowsPerGroup; ++q) {
-            acc[q] = 0.f;
-            comp[q] = 0.f;
-        }
-        for (uint32_t off = lig; off < longest; off += kUnroll * g) {
-            uint32_t t[kUnroll][kRowsPerGroup];
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
-#pragma unroll
-                for (int q = 0; q < kRowsPerGroup; ++q) {
-                    const uint32_t j = rs[q] + off + u * g;
-                    t[u][q] = j < re[q] ? ld_stream(ptgt + j) : 0xFFFFFFFFu;
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < kUnroll; ++u) {
-#pragma unroll
-                for (int q = 0; q < kRowsPerGroup; ++q) {
-                    if (t[u][q] != 0xFFFFFFFFu) kahan_add(acc[q], comp[q], __ldg(contrib_in + t[u][q]));
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kRowsPerGroup; ++q) {
-            const uint32_t row = first + q * groups + group;
-            const double v = group_sum(static_cast<double>(acc[q]) - static_cast<double>(comp[q]), log2g);
-            if (lig == 0 && row < ph.row_end) {
-                double d = 0.0, g = 0.0;
-                pr_finish_row(row, v, re[q] - rs[q], rank_in, rank_out, contrib_out, outdeg, tele, base, damp,
-                              spread, dangling, d, g);
-                my_diff += to_fixed(d);
-                my_dangle += to_fixed(g);
-            }
-        }
-    } else {
-        // Rows without entries: the teleport and dangling share only.
-        const uint32_t row = ph.row_begin + (b - ph.first_block) * kPrThreads + threadIdx.x;
-        if (row < ph.row_end) {
-            double d = 0.0, g = 0.0;
-            pr_finish_row(row, 0.0, 0, rank_in, rank_out, contrib_out, outdeg, tele, base, damp, spread, dangling,
-                          d, g);
-            my_diff += to_fixed(d);
-            my_dangle += to_fixed(g);
-        }
-    }
-    }
-    }
-    unsigned long long* qscratch = reinterpret_cast<unsigned long long*>(scratch);
-    my_diff = block_sum(my_diff, qscratch);
-    my_dangle = block_sum(my_dangle, qscratch);
+    // Loop invariants and the per-warp fixed-point sums live in shared memory,
+    // so that the unrolled gather loop keeps its 8 loads in flight within 32
+    // registers.
+    constexpr int kWarps = kPrThreads / 32;
+    __shared__ double s_mass[2];                     // dangling mass, its uniform share
+    __shared__ unsigned long long s_sum[2 * kWarps];  // per warp: L1 change, dangling mass of r'
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) {
-        row_partials[2 * blockIdx.x] = my_diff;
-        row_partials[2 * blockIdx.x + 1] = my_dangle;
+        s_mass[0] = state->dangling;
+        s_mass[1] = state->dangling / static_cast<double>(V);
+    }
+    if (threadIdx.x < 2 * kWarps) s_sum[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t total_warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t first_unit = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    {
+        for (uint32_t b = first_unit; b < sched.total_blocks; b += total_warps) {
+            uint32_t pi = 0;
+            while (pi + 1 < sched.nphases && sched.phase[pi + 1].first_block <= b) ++pi;
+            const PrPhase ph = sched.phase[pi];
+            if (ph.kind == kPhaseLong) {
+                // One segment of a long row: 32 entries per lane, 8 loads in flight.
+                const uint2 unit = units[b - ph.first_block];
+                const uint32_t row_start = poff[unit.x], row_end = poff[unit.x + 1];
+                const uint32_t s0 = row_start + unit.y * kSegment;
+                const uint32_t s1 = min(s0 + kSegment, row_end);
+                float acc = 0.f, comp = 0.f;
+                uint32_t j = s0 + lane;
+                for (; j + 7 * 32 < s1; j += 8 * 32) {
+                    uint32_t t[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) t[q] = ld_stream(ptgt + j + q * 32);
+                    float c[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) c[q] = __ldg(contrib_in + t[q]);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) kahan_add(acc, comp, c[q]);
+                }
+                for (; j < s1; j += 32) kahan_add(acc, comp, __ldg(contrib_in + ld_stream(ptgt + j)));
+                const double part = warp_sum(static_cast<double>(acc) - static_cast<double>(comp));
+                if (lane == 0) seg_partial[b - ph.first_block] = part;
+            } else if (ph.kind == kPhaseGroup) {
+                // Rows of one class, 2^log2g lanes per row, kRowsPerGroup rows per
+                // group worked on in lockstep: each step issues one target load and
+                // one gather per row (8 in flight per lane with the kUnroll-step
+                // unroll), so no row waits on the previous one's memory round trips.
+                const uint32_t log2g = ph.log2g, g = 1u << log2g;
+                const uint32_t groups = 32u >> log2g;
+                const uint32_t group = lane >> log2g, lig = lane & (g - 1);
+                const uint32_t first = ph.row_begin + (b - ph.first_block) * groups * kRowsPerGroup;
+                uint32_t rs[kRowsPerGroup], re[kRowsPerGroup];
+                uint32_t longest = 0;
+#pragma unroll
+                for (int q = 0; q < kRowsPerGroup; ++q) {
+                    const uint32_t row = first + q * groups + group;
+                    rs[q] = 0;
+                    re[q] = 0;
+                    if (row < ph.row_end) {
+                        rs[q] = poff[row];
+                        re[q] = poff[row + 1];
+                    }
+                    longest = max(longest, re[q] - rs[q]);
+                }
+                float acc[kRowsPerGroup], comp[kRowsPerGroup];
+#pragma unroll
+                for (int q = 0; q < kRowsPerGroup; ++q) {
+                    acc[q] = 0.f;
+                    comp[q] = 0.f;
+                }
+                for (uint32_t off = lig; off < longest; off += kUnroll * g) {
+                    uint32_t t[kUnroll][kRowsPerGroup];
+#pragma unroll
+                    for (int u = 0; u < kUnroll; ++u) {
+#pragma unroll
+                        for (int q = 0; q < kRowsPerGroup; ++q) {
+                            const uint32_t j = rs[q] + off + u * g;
+                            t[u][q] = j < re[q] ? ld_stream(ptgt + j) : 0xFFFFFFFFu;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kUnroll; ++u) {
+#pragma unroll
+                        for (int q = 0; q < kRowsPerGroup; ++q) {
+                            if (t[u][q] != 0xFFFFFFFFu) kahan_add(acc[q], comp[q], __ldg(contrib_in + t[u][q]));
+                        }
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < kRowsPerGroup; ++q) {
+                    const uint32_t row = first + q * groups + group;
+                    const double v = group_sum(static_cast<double>(acc[q]) - static_cast<double>(comp[q]), log2g);
+                    if (lig == 0 && row < ph.row_end) {
+                        double d = 0.0, dg = 0.0;
+                        pr_finish_row(row, v, re[q] - rs[q], rank_in, rank_out, contrib_out, outdeg, tele, base,
+                                      damp, s_mass[1], s_mass[0], d, dg);
+                        atomicAdd(&s_sum[2 * warp], to_fixed(d));
+                        if (dg != 0.0) atomicAdd(&s_sum[2 * warp + 1], to_fixed(dg));
+                    }
+                }
+            } else {
+                // Rows without entries: the teleport and dangling share only.
+                const uint32_t row = ph.row_begin + (b - ph.first_block) * 32 + lane;
+                if (row < ph.row_end) {
+                    double d = 0.0, dg = 0.0;
+                    pr_finish_row(row, 0.0, 0, rank_in, rank_out, contrib_out, outdeg, tele, base, damp, s_mass[1],
+                                  s_mass[0], d, dg);
+                    atomicAdd(&s_sum[2 * warp], to_fixed(d));
+                    if (dg != 0.0) atomicAdd(&s_sum[2 * warp + 1], to_fixed(dg));
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long diff = 0, dangle = 0;
+        for (int w = 0; w < kWarps; ++w) {
+            diff += s_sum[2 * w];
+            dangle += s_sum[2 * w + 1];
+        }
+        row_partials[2 * blockIdx.x] = diff;
+        row_partials[2 * blockIdx.x + 1] = dangle;
     }
 }
 
@@ -456,7 +461,7 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(
     float* __restrict__ contrib_out, const uint32_t* __restrict__ outdeg, const float* __restrict__ tele, uint32_t V,
     double base, double damp, PrState* __restrict__ state,
     double tolerance, const unsigned long long* __restrict__ row_partials, uint32_t row_blocks,
-    unsigned long long* __restrict__ fin_partials, uint32_t* __restrict__ next_chunk) {
+    unsigned long long* __restrict__ fin_partials) {
     if (state->done) return;
     __shared__ unsigned long long scratch[32];
     __shared__ bool s_last;
@@ -503,7 +508,6 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(
         state->dangling = from_fixed(gg);
         if (diff < tolerance) state->done = 1;
         state->ticket = 0;
-        *next_chunk = 0;  // the next iteration's row kernel starts its handout again
     }
 }
 
@@ -614,66 +618,14 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
         // Class c (degrees [2^(c-1), 2^c)): 2^(c-1) lanes per row up to a warp.
         const uint32_t rows = end[c] - begin[c];
         const uint32_t log2g = std::min<uint32_t>(static_cast<uint32_t>(c - 1), 5);
-        const uint32_t per_block = (kPrThreads >> log2g) * kRowsPerGroup;
-        add(kPhaseGroup, begin[c], end[c], log2g, kRowsPerGroup, static_cast<uint32_t>(ceil_div_u64(rows, per_block)));
+        const uint32_t per_unit = (32u >> log2g) * kRowsPerGroup;  // one warp's rows
+        add(kPhaseGroup, begin[c], end[c], log2g, kRowsPerGroup, static_cast<uint32_t>(ceil_div_u64(rows, per_unit)));
     }
-    add(kPhaseEmpty, begin[0], end[0], 0, 0, static_cast<uint32_t>(ceil_div_u64(p.empty_rows, kPrThreads)));
+    add(kPhaseEmpty, begin[0], end[0], 0, 0, static_cast<uint32_t>(ceil_div_u64(p.empty_rows, 32)));
     s.total_blocks = blocks;
-    p.row_ctas = std::max<uint32_t>(1, std::min<uint32_t>(blocks, static_cast<uint32_t>(dev.sm_count) * kRowCtasPerSm));
+    p.row_ctas = std::max<uint32_t>(
+        1, std::min<uint32_t>(ceil_div_u64(blocks, kPrThreads / 32), static_cast<uint32_t>(dev.sm_count) * kRowCtasPerSm));
 
-    // 5. Dispatch chunks: consecutive blocks grouped until their estimated work
-    // (entries plus a fixed cost per block) reaches kChunkWork, then ordered
-    // heaviest first so that the long poles start early.
-    {
-        constexpr uint64_t kBlockCost = 256, kChunkWork = 8192;
-        std::vector<uint32_t> hoff(static_cast<size_t>(V) + 1);
-        GCU_CUDA(cudaMemcpyAsync(hoff.data(), p.poff.ptr, sizeof(uint32_t) * hoff.size(), cudaMemcpyDeviceToHost,
-                                 dev.stream),
-                 "copy");
-        GCU_TRY(dev.sync());
-        auto block_work = [&](uint32_t b) -> uint64_t {
-            uint32_t pi = 0;
-            while (pi + 1 < s.nphases && s.phase[pi + 1].first_block <= b) ++pi;
-            const PrPhase& ph = s.phase[pi];
-            uint64_t entries = 0;
-            if (ph.kind == kPhaseLong) {
-                const uint2 u = units[b - ph.first_block];
-                const uint32_t deg = hoff[u.x + 1] - hoff[u.x];
-                entries = std::min<uint64_t>(kSegment, deg - u.y * kSegment);
-            } else if (ph.kind == kPhaseGroup) {
-                const uint64_t per_block = (kPrThreads >> ph.log2g) * static_cast<uint64_t>(kRowsPerGroup);
-                const uint64_t lo = ph.row_begin + (b - ph.first_block) * per_block;
-                const uint64_t hi = std::min<uint64_t>(lo + per_block, ph.row_end);
-                entries = hoff[hi] - hoff[lo];
-            }
-            return entries + kBlockCost;
-        };
-        std::vector<std::pair<uint64_t, uint2>> list;
-        uint32_t first = 0;
-        uint64_t work = 0;
-        for (uint32_t b = 0; b < blocks; ++b) {
-            work += block_work(b);
-            if (work >= kChunkWork || b + 1 == blocks) {
-                list.push_back({work, make_uint2(first, b + 1)});
-                first = b + 1;
-                work = 0;
-            }
-        }
-        std::stable_sort(list.begin(), list.end(),
-                         [](const std::pair<uint64_t, uint2>& x, const std::pair<uint64_t, uint2>& y) {
-                             return x.first > y.first;
-                         });
-        std::vector<uint2> chunks(list.size());
-        for (size_t i = 0; i < list.size(); ++i) chunks[i] = list[i].second;
-        p.nchunks = static_cast<uint32_t>(chunks.size());
-        GCU_TRY(p.chunks.allocate(dev, std::max<size_t>(chunks.size(), 1)));
-        GCU_TRY(p.next_chunk.allocate(dev, 1));
-        if (!chunks.empty())
-            GCU_CUDA(cudaMemcpyAsync(p.chunks.ptr, chunks.data(), sizeof(uint2) * chunks.size(),
-                                     cudaMemcpyHostToDevice, dev.stream),
-                     "copy");
-        GCU_TRY(dev.sync());  // the host vectors above go out of scope
-    }
     p.fin_blocks = static_cast<uint32_t>(
         std::max<uint64_t>({1, ceil_div_u64(p.long_rows, 256), ceil_div_u64(p.row_ctas, kFinSlice)}));
 
@@ -743,7 +695,6 @@ Error pagerank_ex(GraphImpl& g, bool directed, const float* tele_host, float dam
     init.last_diff = INFINITY;
     *p.host_state = init;
     GCU_CUDA(cudaMemcpyAsync(p.state.ptr, p.host_state, sizeof(PrState), cudaMemcpyHostToDevice, dev.stream), "copy");
-    GCU_CUDA(cudaMemsetAsync(p.next_chunk.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
 
     const double damp = static_cast<double>(damping);
     const double base = (1.0 - damp) / static_cast<double>(V);
@@ -765,12 +716,10 @@ Error pagerank_ex(GraphImpl& g, bool directed, const float* tele_host, float dam
             err = [&]() -> Error {
                 GCU_LAUNCH(dev, "pr_rows", pr_rows_kernel, p.row_ctas, kPrThreads, 0, p.poff.ptr, p.ptgt.ptr,
                            ranks[in], contrib[in], ranks[out], contrib[out], outdeg, d_tele, V, base, damp,
-                           p.state.ptr, p.sched, p.units.ptr, p.seg_partial.ptr, p.row_partials.ptr,
-                           p.chunks.ptr, p.nchunks, p.next_chunk.ptr);
+                           p.state.ptr, p.sched, p.units.ptr, p.seg_partial.ptr, p.row_partials.ptr);
                 GCU_LAUNCH(dev, "pr_finish", pr_finish_kernel, p.fin_blocks, 256, 0, p.poff.ptr, p.long_rows,
                            p.unit_begin.ptr, p.seg_partial.ptr, ranks[in], ranks[out], contrib[out], outdeg, d_tele,
-                           V, base, damp, p.state.ptr, tol, p.row_partials.ptr, p.row_ctas, p.fin_partials.ptr,
-                           p.next_chunk.ptr);
+                           V, base, damp, p.state.ptr, tol, p.row_partials.ptr, p.row_ctas, p.fin_partials.ptr);
                 return ok();
             }();
         }

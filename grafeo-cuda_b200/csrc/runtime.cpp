@@ -156,6 +156,8 @@ GraphImpl::~GraphImpl() {
         destroy_pagerank_plan(pr_plan);
         destroy_pagerank_plan(pr_plan_directed);
         destroy_bfs_work(bfs_work);
+        destroy_kt_cache(kt_cache);
+        kt_cache = nullptr;
         pr_plan = nullptr;
         pr_plan_directed = nullptr;
         bfs_work = nullptr;

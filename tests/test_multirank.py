@@ -31,7 +31,9 @@ rank = d.rank
 d.barrier()
 mx = d.max(10.0 + rank)
 sm = d.sum(1.0 + rank)
-print(json.dumps({"rank": rank, "world": d.world, "max": mx, "sum": sm}), flush=True)
+# One file per rank: two ranks printing to one pipe can interleave their lines.
+with open(os.path.join(os.environ["OUT_DIR"], f"rank{rank}.json"), "w") as fh:
+    json.dump({"rank": rank, "world": d.world, "max": mx, "sum": sm}, fh)
 d.close()
 """
 
@@ -57,9 +59,9 @@ def run_torchrun(args, env_extra=None, timeout=300):
 def test_dist_max_and_sum_over_two_gloo_ranks(tmp_path):
     script = tmp_path / "worker.py"
     script.write_text(WORKER)
-    r = run_torchrun([str(script)])
+    r = run_torchrun([str(script)], env_extra={"OUT_DIR": str(tmp_path)})
     assert r.returncode == 0, r.stderr[-2000:]
-    lines = [json.loads(line) for line in r.stdout.splitlines() if line.startswith("{")]
+    lines = [json.loads((tmp_path / f"rank{k}.json").read_text()) for k in (0, 1)]
     assert sorted(x["rank"] for x in lines) == [0, 1]
     for x in lines:
         assert x["world"] == 2 and x["max"] == 11.0 and x["sum"] == 3.0
