@@ -8,9 +8,9 @@
 //
 //  1. Orientation: each undirected edge is kept once, from the endpoint of
 //     lower (degree, id) to the higher one, the same rule as
-//     from_edge_pairs_oriented (csr_export.rs:319-329). A count pass, a device
-//     scan and an order-preserving fill pass build the DAG CSR; self-loops
-//     drop out because the order is strict. Max out-degree becomes O(sqrt m).
+//     from_edge_pairs_oriented (csr_export.rs:319-329). A flag pass over the
+//     flat entry range, a device scan and an order-preserving scatter build
+//     the DAG CSR; self-loops drop out because the order is strict. Max out-degree becomes O(sqrt m).
 //     A CSR that is not symmetric is oriented by id alone (keep v > u): the
 //     count below is then exactly the reference's formula, the sum over
 //     entries u -> v, v > u, of |{w in N(u) ∩ N(v) : w > v}|
@@ -40,81 +40,116 @@ __device__ __forceinline__ bool dag_keep(uint32_t u, uint32_t du, uint32_t v, ui
     return by_degree ? (du < dv || (du == dv && u < v)) : u < v;
 }
 
-// Pass 1: out-degree of every vertex in the degree-oriented DAG.
-__global__ void __launch_bounds__(256) tc_orient_count_kernel(const uint32_t* __restrict__ offsets,
-                                                              const uint32_t* __restrict__ targets, uint32_t V,
-                                                              bool by_degree, uint32_t* __restrict__ out_deg) {
-    const unsigned lane = lane_id();
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
-        const uint32_t count = static_cast<uint32_t>(min_u64(32, V - base));
-        uint32_t s = 0, e = 0;
-        if (lane < count) {
-            s = offsets[base + lane];
-            e = offsets[base + lane + 1];
+// The orientation runs over the flat range of CSR entries, so a hub's list is
+// shared by many blocks instead of walked by one warp:
+//  1. keep[j] for every entry j = u -> v (tc_orient_flag_kernel): a block
+//     takes a tile of consecutive entries, finds their rows with a binary
+//     search of the row starts staged in shared memory, and evaluates the
+//     orientation rule;
+//  2. an exclusive scan of keep gives every kept entry its DAG position (the
+//     DAG lists are the CSR lists filtered, in the same order);
+//  3. the kept entries are scattered to their positions and every row's DAG
+//     offset is the scan at the row's first CSR entry.
+constexpr int kOrientThreads = 256;
+constexpr int kOrientItems = 4;
+constexpr int kOrientTile = kOrientThreads * kOrientItems;  // entries per tile
+
+// Row of every entry of the tile [e0, e1) via the staged row starts (rows
+// r0 .. r0 + nrows - 1 cover the tile, empty rows included); falls back to a
+// search of the global offsets when the tile spans more rows than fit.
+__device__ __forceinline__ uint32_t tile_row(const uint32_t* __restrict__ offsets, uint32_t V, const uint32_t* s_start,
+                                             bool staged, uint32_t r0, uint32_t nrows, uint32_t j) {
+    if (!staged) return row_of_entry(offsets, V, j);
+    uint32_t lo = 0, hi = nrows;  // largest k with s_start[k] <= j
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_start[mid] <= j)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return r0 + lo;
+}
+
+// Stages the row starts of the tile [e0, e1) in shared memory; returns
+// whether they fit (s_meta = {r0, nrows}).
+__device__ __forceinline__ bool stage_tile_rows(const uint32_t* __restrict__ offsets, uint32_t V, uint64_t e0,
+                                                uint64_t e1, uint32_t* s_start, uint32_t* s_meta) {
+    if (threadIdx.x < 2)
+        s_meta[threadIdx.x] = row_of_entry(offsets, V, static_cast<uint32_t>(threadIdx.x == 0 ? e0 : e1 - 1));
+    __syncthreads();
+    const uint32_t r0 = s_meta[0], nrows = s_meta[1] - r0 + 1;
+    const bool staged = nrows <= kOrientTile;
+    if (staged)
+        for (uint32_t k = threadIdx.x; k < nrows; k += blockDim.x) s_start[k] = offsets[r0 + k];
+    __syncthreads();
+    return staged;
+}
+
+__global__ void __launch_bounds__(kOrientThreads) tc_orient_flag_kernel(const uint32_t* __restrict__ offsets,
+                                                                        const uint32_t* __restrict__ targets,
+                                                                        uint32_t V, uint32_t E, bool by_degree,
+                                                                        uint32_t* __restrict__ keep) {
+    __shared__ uint32_t s_start[kOrientTile];
+    __shared__ uint32_t s_meta[2];
+    for (uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kOrientTile; e0 < E;
+         e0 += static_cast<uint64_t>(gridDim.x) * kOrientTile) {
+        const uint64_t e1 = min_u64(e0 + kOrientTile, E);
+        const bool staged = stage_tile_rows(offsets, V, e0, e1, s_start, s_meta);
+        const uint32_t r0 = s_meta[0], nrows = s_meta[1] - r0 + 1;
+#pragma unroll
+        for (int q = 0; q < kOrientItems; ++q) {
+            const uint64_t j = e0 + q * kOrientThreads + threadIdx.x;
+            if (j >= e1) continue;
+            const uint32_t u = tile_row(offsets, V, s_start, staged, r0, nrows, static_cast<uint32_t>(j));
+            const uint32_t du = __ldg(offsets + u + 1) - __ldg(offsets + u);
+            const uint32_t v = ld_stream(targets + j);
+            const uint32_t dv = __ldg(offsets + v + 1) - __ldg(offsets + v);
+            keep[j] = dag_keep(u, du, v, dv, by_degree) ? 1u : 0u;
         }
-        uint32_t mine = 0;
-        for (uint32_t i = 0; i < count; ++i) {
-            const uint32_t u = static_cast<uint32_t>(base + i);
-            const uint32_t start = __shfl_sync(kFullMask, s, i), end = __shfl_sync(kFullMask, e, i);
-            const uint32_t du = end - start;
-            uint32_t kept = 0;
-            for (uint32_t j = start + lane; j < end; j += 32) {
-                const uint32_t v = ld_stream(targets + j);
-                const uint32_t dv = __ldg(offsets + v + 1) - __ldg(offsets + v);
-                kept += dag_keep(u, du, v, dv, by_degree) ? 1u : 0u;
-            }
-            kept = warp_sum(kept);
-            if (lane == i) mine = kept;
-        }
-        if (lane < count) out_deg[base + lane] = mine;
+        __syncthreads();  // the staged starts are rewritten for the next tile
     }
 }
 
-// Pass 2: write the kept neighbours in list order (still sorted by id).
-__global__ void __launch_bounds__(256) tc_orient_fill_kernel(const uint32_t* __restrict__ offsets,
-                                                             const uint32_t* __restrict__ targets, uint32_t V,
-                                                             bool by_degree, const uint32_t* __restrict__ dag_offsets,
-                                                             uint32_t* __restrict__ dag_targets,
-                                                             const uint32_t* __restrict__ rev,
-                                                             uint32_t* __restrict__ dag_eid) {
-    const unsigned lane = lane_id();
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
-        const uint32_t count = static_cast<uint32_t>(min_u64(32, V - base));
-        uint32_t s = 0, e = 0, o = 0;
-        if (lane < count) {
-            s = offsets[base + lane];
-            e = offsets[base + lane + 1];
-            o = dag_offsets[base + lane];
-        }
-        for (uint32_t i = 0; i < count; ++i) {
-            const uint32_t u = static_cast<uint32_t>(base + i);
-            const uint32_t start = __shfl_sync(kFullMask, s, i), end = __shfl_sync(kFullMask, e, i);
-            uint32_t out = __shfl_sync(kFullMask, o, i);
-            const uint32_t du = end - start;
-            for (uint32_t j0 = start; j0 < end; j0 += 32) {
-                const uint32_t j = j0 + lane;
-                bool keep = false;
-                uint32_t v = 0;
-                if (j < end) {
-                    v = ld_stream(targets + j);
-                    const uint32_t dv = __ldg(offsets + v + 1) - __ldg(offsets + v);
-                    keep = dag_keep(u, du, v, dv, by_degree);
-                }
-                const unsigned mask = __ballot_sync(kFullMask, keep);
-                if (keep) {
-                    const uint32_t at = out + __popc(mask & ((1u << lane) - 1));
-                    dag_targets[at] = v;
-                    // Undirected edge id: the CSR index of its u < v entry.
-                    if (dag_eid) dag_eid[at] = u < v ? j : rev[j];
-                }
-                out += __popc(mask);
+// Kept entries to their DAG positions; with dag_eid, also the CSR index of
+// the edge's u < v entry (the undirected edge id).
+__global__ void __launch_bounds__(kOrientThreads) tc_orient_fill_kernel(const uint32_t* __restrict__ offsets,
+                                                                        const uint32_t* __restrict__ targets,
+                                                                        uint32_t V, uint32_t E,
+                                                                        const uint32_t* __restrict__ pos,
+                                                                        uint32_t* __restrict__ dag_targets,
+                                                                        const uint32_t* __restrict__ rev,
+                                                                        uint32_t* __restrict__ dag_eid) {
+    __shared__ uint32_t s_start[kOrientTile];
+    __shared__ uint32_t s_meta[2];
+    for (uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kOrientTile; e0 < E;
+         e0 += static_cast<uint64_t>(gridDim.x) * kOrientTile) {
+        const uint64_t e1 = min_u64(e0 + kOrientTile, E);
+        const bool staged = dag_eid ? stage_tile_rows(offsets, V, e0, e1, s_start, s_meta) : false;
+        const uint32_t r0 = dag_eid ? s_meta[0] : 0, nrows = dag_eid ? s_meta[1] - r0 + 1 : 0;
+#pragma unroll
+        for (int q = 0; q < kOrientItems; ++q) {
+            const uint64_t j = e0 + q * kOrientThreads + threadIdx.x;
+            if (j >= e1) continue;
+            const uint32_t at = pos[j];
+            if (pos[j + 1] == at) continue;
+            const uint32_t v = ld_stream(targets + j);
+            dag_targets[at] = v;
+            if (dag_eid) {
+                const uint32_t u = tile_row(offsets, V, s_start, staged, r0, nrows, static_cast<uint32_t>(j));
+                dag_eid[at] = u < v ? static_cast<uint32_t>(j) : rev[j];
             }
         }
+        if (dag_eid) __syncthreads();
     }
+}
+
+// dag_offsets[u] = pos[offsets[u]] for u = 0..V.
+__global__ void tc_orient_offsets_kernel(const uint32_t* __restrict__ offsets, uint32_t V,
+                                         const uint32_t* __restrict__ pos, uint32_t* __restrict__ dag_offsets) {
+    for (uint64_t u = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u <= V;
+         u += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        dag_offsets[u] = pos[offsets[u]];
 }
 
 // ---------------------------------------------------------------- host
@@ -139,21 +174,28 @@ struct CountSink {
 Error build_dag(GraphImpl& g, bool by_degree, const uint32_t* rev, DeviceBuffer<uint32_t>* dag_offsets,
                 DeviceBuffer<uint32_t>* dag_targets, DeviceBuffer<uint32_t>* dag_eid, uint32_t* m) {
     DeviceImpl& dev = *g.dev;
-    const uint32_t V = g.num_nodes;
+    const uint32_t V = g.num_nodes, E = g.num_edges;
     GCU_TRY(dag_offsets->allocate(dev, static_cast<uint64_t>(V) + 1));
-    const unsigned grid = static_cast<unsigned>(
-        std::min<uint64_t>(ceil_div_u64(ceil_div_u64(V, 32) * 32, 256), static_cast<uint64_t>(dev.sm_count) * 16));
-    GCU_LAUNCH(dev, "tc_orient_count", tc_orient_count_kernel, grid, 256, 0, g.offsets.ptr, g.targets.ptr, V,
-               by_degree, dag_offsets->ptr);
-    GCU_TRY(exclusive_scan_u32(dev, dag_offsets->ptr, dag_offsets->ptr, V));
     *m = 0;
-    GCU_CUDA(cudaMemcpyAsync(m, dag_offsets->ptr + V, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+    DeviceBuffer<uint32_t> pos;  // keep flags, then their exclusive scan (E + 1)
+    GCU_TRY(pos.allocate(dev, static_cast<uint64_t>(E) + 1));
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned tiles = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(E, kOrientTile), cap)));
+    const unsigned vgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(static_cast<uint64_t>(V) + 1, 256), cap));
+    if (E > 0)
+        GCU_LAUNCH(dev, "tc_orient_flag", tc_orient_flag_kernel, tiles, kOrientThreads, 0, g.offsets.ptr,
+                   g.targets.ptr, V, E, by_degree, pos.ptr);
+    GCU_TRY(exclusive_scan_u32(dev, pos.ptr, pos.ptr, E));
+    GCU_LAUNCH(dev, "tc_orient_offsets", tc_orient_offsets_kernel, vgrid, 256, 0, g.offsets.ptr, V, pos.ptr,
+               dag_offsets->ptr);
+    GCU_CUDA(cudaMemcpyAsync(m, pos.ptr + E, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
     GCU_TRY(dev.sync());
     GCU_TRY(dag_targets->allocate(dev, std::max<uint32_t>(*m, 1)));
     if (dag_eid) GCU_TRY(dag_eid->allocate(dev, std::max<uint32_t>(*m, 1)));
     if (*m == 0) return ok();
-    GCU_LAUNCH(dev, "tc_orient_fill", tc_orient_fill_kernel, grid, 256, 0, g.offsets.ptr, g.targets.ptr, V, by_degree,
-               dag_offsets->ptr, dag_targets->ptr, rev, dag_eid ? dag_eid->ptr : nullptr);
+    GCU_LAUNCH(dev, "tc_orient_fill", tc_orient_fill_kernel, tiles, kOrientThreads, 0, g.offsets.ptr, g.targets.ptr,
+               V, E, pos.ptr, dag_targets->ptr, rev, dag_eid ? dag_eid->ptr : nullptr);
+    GCU_TRY(dev.sync());  // pos is freed on return
     return ok();
 }
 
