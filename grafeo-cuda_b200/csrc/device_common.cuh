@@ -99,8 +99,68 @@ __device__ __forceinline__ uint32_t row_of_entry(const uint32_t* offsets, uint32
     return lo;
 }
 
+// ---------------------------------------------------------------- entry tiles
+// A block that works on a tile of consecutive CSR entries [e0, e1) finds the
+// row of each entry from the row starts of the tile, staged in shared memory
+// (s_start, kTile words; s_meta, 2 words); when the tile spans more rows than
+// fit (runs of empty rows), each entry searches the global offsets instead.
+
+// Largest row r in [0, n) with offsets[r] <= pos (defined above) picks, among
+// empty rows that share a start, the non-empty row that holds the entry.
+template <int kTile>
+__device__ __forceinline__ bool stage_tile_rows(const uint32_t* __restrict__ offsets, uint32_t V, uint64_t e0,
+                                                uint64_t e1, uint32_t* s_start, uint32_t* s_meta) {
+    if (threadIdx.x < 2)
+        s_meta[threadIdx.x] = row_of_entry(offsets, V, static_cast<uint32_t>(threadIdx.x == 0 ? e0 : e1 - 1));
+    __syncthreads();
+    const uint32_t r0 = s_meta[0], nrows = s_meta[1] - r0 + 1;
+    const bool staged = nrows <= static_cast<uint32_t>(kTile);
+    if (staged)
+        for (uint32_t k = threadIdx.x; k < nrows; k += blockDim.x) s_start[k] = offsets[r0 + k];
+    __syncthreads();
+    return staged;
+}
+
+__device__ __forceinline__ uint32_t tile_row(const uint32_t* __restrict__ offsets, uint32_t V, const uint32_t* s_start,
+                                             bool staged, uint32_t r0, uint32_t nrows, uint32_t j) {
+    if (!staged) return row_of_entry(offsets, V, j);
+    uint32_t lo = 0, hi = nrows;  // largest k with s_start[k] <= j
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (s_start[mid] <= j)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return r0 + lo;
+}
+
 __host__ __device__ __forceinline__ uint64_t min_u64(uint64_t a, uint64_t b) { return a < b ? a : b; }
 
 __host__ __device__ __forceinline__ uint64_t ceil_div_u64(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+// Calls f(j, row) for every entry j of a CSR with V rows and E entries: each
+// block takes tiles of kThreads * kItems consecutive entries (grid-stride),
+// so long rows are shared by many blocks and every access to the entries is
+// coalesced. All threads of the block must call it.
+template <int kThreads, int kItems, class F>
+__device__ __forceinline__ void for_each_entry(const uint32_t* __restrict__ offsets, uint32_t V, uint64_t E, F f) {
+    constexpr int kTile = kThreads * kItems;
+    __shared__ uint32_t s_start[kTile];
+    __shared__ uint32_t s_meta[2];
+    for (uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kTile; e0 < E;
+         e0 += static_cast<uint64_t>(gridDim.x) * kTile) {
+        const uint64_t e1 = min_u64(e0 + kTile, E);
+        const bool staged = stage_tile_rows<kTile>(offsets, V, e0, e1, s_start, s_meta);
+        const uint32_t r0 = s_meta[0], nrows = s_meta[1] - r0 + 1;
+#pragma unroll
+        for (int q = 0; q < kItems; ++q) {
+            const uint64_t j = e0 + q * kThreads + threadIdx.x;
+            if (j < e1) f(static_cast<uint32_t>(j), tile_row(offsets, V, s_start, staged, r0, nrows,
+                                                              static_cast<uint32_t>(j)));
+        }
+        __syncthreads();  // the staged starts are rewritten for the next tile
+    }
+}
 
 }  // namespace gcu

@@ -35,24 +35,10 @@ namespace gcu {
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 
-// src[j] = row of entry j (a warp per 32 rows, coalesced writes).
-__global__ void __launch_bounds__(256) kt_rows_kernel(const uint32_t* __restrict__ offsets, uint32_t V,
+// src[j] = row of entry j.
+__global__ void __launch_bounds__(256) kt_rows_kernel(const uint32_t* __restrict__ offsets, uint32_t V, uint32_t E,
                                                       uint32_t* __restrict__ src) {
-    const unsigned lane = lane_id();
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
-        const uint32_t count = static_cast<uint32_t>(min_u64(32, V - base));
-        uint32_t s = 0, e = 0;
-        if (lane < count) {
-            s = offsets[base + lane];
-            e = offsets[base + lane + 1];
-        }
-        for (uint32_t i = 0; i < count; ++i) {
-            const uint32_t start = __shfl_sync(kFullMask, s, i), end = __shfl_sync(kFullMask, e, i);
-            for (uint32_t j = start + lane; j < end; j += 32) src[j] = static_cast<uint32_t>(base + i);
-        }
-    }
+    for_each_entry<256, 4>(offsets, V, E, [&](uint32_t j, uint32_t row) { src[j] = row; });
 }
 
 // rev[j] = index of entry v -> u for entry j = u -> v, or kNone.
@@ -364,9 +350,9 @@ static Error ensure_kt_cache(GraphImpl& g, KtCache** out) {
         DeviceBuffer<uint32_t> count;
         GCU_TRY(count.allocate(dev, 1));
         const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
-        const unsigned row_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
+        const unsigned tile_grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(E, 1024), cap)));
         const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
-        GCU_LAUNCH(dev, "kt_rows", kt_rows_kernel, row_grid, 256, 0, g.offsets.ptr, V, c->src.ptr);
+        GCU_LAUNCH(dev, "kt_rows", kt_rows_kernel, tile_grid, 256, 0, g.offsets.ptr, V, E, c->src.ptr);
         GCU_LAUNCH(dev, "kt_reverse", kt_reverse_kernel, edge_grid, 256, 0, g.offsets.ptr, g.targets.ptr, c->src.ptr,
                    E, c->rev.ptr);
         GCU_CUDA(cudaMemsetAsync(c->loop.ptr, 0, V, dev.stream), "memset");
@@ -446,9 +432,9 @@ Error k_truss(GraphImpl& g, uint32_t k, std::vector<uint32_t>* edges, uint32_t* 
     GCU_TRY(src.allocate(dev, E));
     GCU_TRY(rev.allocate(dev, E));
     const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
-    const unsigned row_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
+    const unsigned tile_grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(E, 1024), cap)));
     const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
-    GCU_LAUNCH(dev, "kt_rows", kt_rows_kernel, row_grid, 256, 0, g.offsets.ptr, V, src.ptr);
+    GCU_LAUNCH(dev, "kt_rows", kt_rows_kernel, tile_grid, 256, 0, g.offsets.ptr, V, E, src.ptr);
     GCU_LAUNCH(dev, "kt_reverse", kt_reverse_kernel, edge_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src.ptr, E,
                rev.ptr);
     return k_truss_general(g, k, src.ptr, rev.ptr, edges, iterations);

@@ -189,31 +189,36 @@ __global__ void pr_perm_degree_kernel(const uint32_t* __restrict__ offsets, cons
     }
 }
 
-// Relabelled row r = original row perm[r] with every target renamed; a warp
-// walks 32 rows, the lanes stride over each row.
-__global__ void __launch_bounds__(256) pr_perm_fill_kernel(const uint32_t* __restrict__ offsets,
-                                                           const uint32_t* __restrict__ targets,
-                                                           const uint32_t* __restrict__ perm,
-                                                           const uint32_t* __restrict__ inv,
-                                                           const uint32_t* __restrict__ poff, uint32_t V,
-                                                           uint32_t* __restrict__ ptgt) {
-    const unsigned lane = lane_id();
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
-        const uint32_t count = static_cast<uint32_t>(min_u64(32, V - base));
-        uint32_t s = 0, e = 0, o = 0;
-        if (lane < count) {
-            const uint32_t u = perm[base + lane];
-            s = offsets[u];
-            e = offsets[u + 1];
-            o = poff[base + lane];
+// Relabelled CSR entry k of row r is original entry offsets[perm[r]] +
+// (k - poff[r]) with its target renamed. Blocks work on tiles of consecutive
+// output entries (rows found through the staged row starts), so a hub's list
+// is copied by many blocks, reads and writes coalesced.
+constexpr int kFillThreads = 256;
+constexpr int kFillItems = 4;
+constexpr int kFillTile = kFillThreads * kFillItems;
+
+__global__ void __launch_bounds__(kFillThreads) pr_perm_fill_kernel(const uint32_t* __restrict__ offsets,
+                                                                    const uint32_t* __restrict__ targets,
+                                                                    const uint32_t* __restrict__ perm,
+                                                                    const uint32_t* __restrict__ inv,
+                                                                    const uint32_t* __restrict__ poff, uint32_t V,
+                                                                    uint32_t E, uint32_t* __restrict__ ptgt) {
+    __shared__ uint32_t s_start[kFillTile];
+    __shared__ uint32_t s_meta[2];
+    for (uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kFillTile; e0 < E;
+         e0 += static_cast<uint64_t>(gridDim.x) * kFillTile) {
+        const uint64_t e1 = min_u64(e0 + kFillTile, E);
+        const bool staged = stage_tile_rows<kFillTile>(poff, V, e0, e1, s_start, s_meta);
+        const uint32_t r0 = s_meta[0], nrows = s_meta[1] - r0 + 1;
+#pragma unroll
+        for (int q = 0; q < kFillItems; ++q) {
+            const uint64_t k = e0 + q * kFillThreads + threadIdx.x;
+            if (k >= e1) continue;
+            const uint32_t r = tile_row(poff, V, s_start, staged, r0, nrows, static_cast<uint32_t>(k));
+            const uint32_t src = offsets[perm[r]] + static_cast<uint32_t>(k - poff[r]);
+            ptgt[k] = inv[ld_stream(targets + src)];
         }
-        for (uint32_t i = 0; i < count; ++i) {
-            const uint32_t start = __shfl_sync(kFullMask, s, i), end = __shfl_sync(kFullMask, e, i);
-            const uint32_t out = __shfl_sync(kFullMask, o, i);
-            for (uint32_t j = start + lane; j < end; j += 32) ptgt[out + (j - start)] = inv[ld_stream(targets + j)];
-        }
+        __syncthreads();  // the staged starts are rewritten for the next tile
     }
 }
 
@@ -549,8 +554,10 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
     GCU_LAUNCH(dev, "pr_perm_degree", pr_perm_degree_kernel, vgrid, 256, 0, pull_offsets, p.perm.ptr, V, p.poff.ptr);
     GCU_TRY(exclusive_scan_u32(dev, p.poff.ptr, p.poff.ptr, V));
     if (E > 0) {
-        GCU_LAUNCH(dev, "pr_perm_fill", pr_perm_fill_kernel, vgrid, 256, 0, pull_offsets, pull_targets, p.perm.ptr,
-                   p.inv.ptr, p.poff.ptr, V, p.ptgt.ptr);
+        const unsigned fill_grid =
+            static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(E, kFillTile), cap)));
+        GCU_LAUNCH(dev, "pr_perm_fill", pr_perm_fill_kernel, fill_grid, kFillThreads, 0, pull_offsets, pull_targets,
+                   p.perm.ptr, p.inv.ptr, p.poff.ptr, V, E, p.ptgt.ptr);
     }
     if (out_offsets) {
         GCU_TRY(p.outdeg.allocate(dev, V));

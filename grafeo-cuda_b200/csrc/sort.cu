@@ -97,36 +97,27 @@ Error radix_sort_u64(DeviceImpl& dev, uint64_t* keys, uint64_t* tmp, uint64_t n,
 
 // ---------------------------------------------------------------- transpose
 
-// keys[j] = (target << 32) | source for every entry j (a warp walks 32 rows).
+// keys[j] = (target << 32) | source for every entry j.
 __global__ void __launch_bounds__(256) transpose_keys_kernel(const uint32_t* __restrict__ offsets,
                                                              const uint32_t* __restrict__ targets, uint32_t V,
-                                                             uint64_t* __restrict__ keys) {
-    const unsigned lane = lane_id();
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
-        const uint32_t count = static_cast<uint32_t>(min_u64(32, V - base));
-        uint32_t s = 0, e = 0;
-        if (lane < count) {
-            s = offsets[base + lane];
-            e = offsets[base + lane + 1];
-        }
-        for (uint32_t i = 0; i < count; ++i) {
-            const uint32_t start = __shfl_sync(kFullMask, s, i), end = __shfl_sync(kFullMask, e, i);
-            const uint64_t u = base + i;
-            for (uint32_t j = start + lane; j < end; j += 32)
-                keys[j] = (static_cast<uint64_t>(targets[j]) << 32) | u;
-        }
-    }
+                                                             uint32_t E, uint64_t* __restrict__ keys) {
+    for_each_entry<256, 4>(offsets, V, E, [&](uint32_t j, uint32_t u) {
+        keys[j] = (static_cast<uint64_t>(targets[j]) << 32) | u;
+    });
 }
 
-__global__ void transpose_split_kernel(const uint64_t* __restrict__ keys, uint32_t E, uint32_t* __restrict__ t_targets,
-                                       uint32_t* __restrict__ in_degree) {
-    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < E;
+// Sorted keys -> transposed lists: t_targets[j] = the source of key j, and
+// in-list v starts at the first key whose target is >= v (rows prev < v <=
+// cur get the boundary between keys j - 1 and j; every row one writer, no
+// atomics on the hubs' in-degrees).
+__global__ void transpose_split_kernel(const uint64_t* __restrict__ keys, uint32_t E, uint32_t V,
+                                       uint32_t* __restrict__ t_targets, uint32_t* __restrict__ t_offsets) {
+    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j <= E;
          j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        const uint64_t k = keys[j];
-        t_targets[j] = static_cast<uint32_t>(k);
-        atomicAdd(in_degree + (k >> 32), 1u);
+        const int64_t prev = j == 0 ? -1 : static_cast<int64_t>(keys[j - 1] >> 32);
+        const int64_t cur = j < E ? static_cast<int64_t>(keys[j] >> 32) : static_cast<int64_t>(V);
+        if (j < E) t_targets[j] = static_cast<uint32_t>(keys[j]);
+        for (int64_t r = prev + 1; r <= cur; ++r) t_offsets[r] = static_cast<uint32_t>(j);
     }
 }
 
@@ -140,17 +131,16 @@ Error transpose_csr(DeviceImpl& dev, const uint32_t* offsets, const uint32_t* ta
     GCU_TRY(keys.allocate(dev, E));
     GCU_TRY(tmp.allocate(dev, E));
     const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
-    const unsigned vgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
-    const unsigned egrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
-    GCU_LAUNCH(dev, "transpose_keys", transpose_keys_kernel, vgrid, 256, 0, offsets, targets, V, keys.ptr);
+    const unsigned tgrid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(E, 1024), cap)));
+    const unsigned egrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(static_cast<uint64_t>(E) + 1, 256), cap));
+    GCU_LAUNCH(dev, "transpose_keys", transpose_keys_kernel, tgrid, 256, 0, offsets, targets, V, E, keys.ptr);
     uint32_t bits = 0;
     while (bits < 32 && (static_cast<uint64_t>(1) << bits) < V) ++bits;
     uint64_t* sorted = nullptr;
     // Stable sort by target only: sources stay ascending inside each in-list.
     GCU_TRY(radix_sort_u64(dev, keys.ptr, tmp.ptr, E, 32, 32 + ((bits + 7) / 8) * 8, &sorted));
-    GCU_LAUNCH(dev, "transpose_split", transpose_split_kernel, egrid, 256, 0, sorted, E, t_targets->ptr,
+    GCU_LAUNCH(dev, "transpose_split", transpose_split_kernel, egrid, 256, 0, sorted, E, V, t_targets->ptr,
                t_offsets->ptr);
-    GCU_TRY(exclusive_scan_u32(dev, t_offsets->ptr, t_offsets->ptr, V));
     GCU_TRY(dev.sync());  // keys/tmp are freed on return
     return ok();
 }

@@ -54,38 +54,6 @@ constexpr int kOrientThreads = 256;
 constexpr int kOrientItems = 4;
 constexpr int kOrientTile = kOrientThreads * kOrientItems;  // entries per tile
 
-// Row of every entry of the tile [e0, e1) via the staged row starts (rows
-// r0 .. r0 + nrows - 1 cover the tile, empty rows included); falls back to a
-// search of the global offsets when the tile spans more rows than fit.
-__device__ __forceinline__ uint32_t tile_row(const uint32_t* __restrict__ offsets, uint32_t V, const uint32_t* s_start,
-                                             bool staged, uint32_t r0, uint32_t nrows, uint32_t j) {
-    if (!staged) return row_of_entry(offsets, V, j);
-    uint32_t lo = 0, hi = nrows;  // largest k with s_start[k] <= j
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (s_start[mid] <= j)
-            lo = mid;
-        else
-            hi = mid;
-    }
-    return r0 + lo;
-}
-
-// Stages the row starts of the tile [e0, e1) in shared memory; returns
-// whether they fit (s_meta = {r0, nrows}).
-__device__ __forceinline__ bool stage_tile_rows(const uint32_t* __restrict__ offsets, uint32_t V, uint64_t e0,
-                                                uint64_t e1, uint32_t* s_start, uint32_t* s_meta) {
-    if (threadIdx.x < 2)
-        s_meta[threadIdx.x] = row_of_entry(offsets, V, static_cast<uint32_t>(threadIdx.x == 0 ? e0 : e1 - 1));
-    __syncthreads();
-    const uint32_t r0 = s_meta[0], nrows = s_meta[1] - r0 + 1;
-    const bool staged = nrows <= kOrientTile;
-    if (staged)
-        for (uint32_t k = threadIdx.x; k < nrows; k += blockDim.x) s_start[k] = offsets[r0 + k];
-    __syncthreads();
-    return staged;
-}
-
 __global__ void __launch_bounds__(kOrientThreads) tc_orient_flag_kernel(const uint32_t* __restrict__ offsets,
                                                                         const uint32_t* __restrict__ targets,
                                                                         uint32_t V, uint32_t E, bool by_degree,
@@ -95,7 +63,7 @@ __global__ void __launch_bounds__(kOrientThreads) tc_orient_flag_kernel(const ui
     for (uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kOrientTile; e0 < E;
          e0 += static_cast<uint64_t>(gridDim.x) * kOrientTile) {
         const uint64_t e1 = min_u64(e0 + kOrientTile, E);
-        const bool staged = stage_tile_rows(offsets, V, e0, e1, s_start, s_meta);
+        const bool staged = stage_tile_rows<kOrientTile>(offsets, V, e0, e1, s_start, s_meta);
         const uint32_t r0 = s_meta[0], nrows = s_meta[1] - r0 + 1;
 #pragma unroll
         for (int q = 0; q < kOrientItems; ++q) {
@@ -125,7 +93,7 @@ __global__ void __launch_bounds__(kOrientThreads) tc_orient_fill_kernel(const ui
     for (uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kOrientTile; e0 < E;
          e0 += static_cast<uint64_t>(gridDim.x) * kOrientTile) {
         const uint64_t e1 = min_u64(e0 + kOrientTile, E);
-        const bool staged = dag_eid ? stage_tile_rows(offsets, V, e0, e1, s_start, s_meta) : false;
+        const bool staged = dag_eid ? stage_tile_rows<kOrientTile>(offsets, V, e0, e1, s_start, s_meta) : false;
         const uint32_t r0 = dag_eid ? s_meta[0] : 0, nrows = dag_eid ? s_meta[1] - r0 + 1 : 0;
 #pragma unroll
         for (int q = 0; q < kOrientItems; ++q) {

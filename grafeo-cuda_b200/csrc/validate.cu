@@ -91,36 +91,20 @@ Error validate_csr_device(DeviceImpl& dev, const uint32_t* d_offsets, const uint
     return ok();
 }
 
-// Symmetry test: every entry u -> v needs v -> u. A warp walks 32 rows; the
-// lanes stride over each row and binary-search u in the neighbour's list.
-__global__ void csr_symmetry_kernel(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
-                                    uint32_t V, uint32_t* __restrict__ asymmetric) {
-    const unsigned lane = lane_id();
-    const uint64_t warp = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t base = warp * 32; base < V; base += nwarps * 32) {
-        const uint32_t count = static_cast<uint32_t>(min_u64(32, V - base));
-        uint32_t s = 0, e = 0;
-        if (lane < count) {
-            s = offsets[base + lane];
-            e = offsets[base + lane + 1];
-        }
-        bool bad = false;
-        for (uint32_t i = 0; i < count; ++i) {
-            const uint32_t u = static_cast<uint32_t>(base + i);
-            const uint32_t start = __shfl_sync(kFullMask, s, i), end = __shfl_sync(kFullMask, e, i);
-            for (uint32_t j = start + lane; j < end; j += 32) {
-                const uint32_t v = targets[j];
-                const uint32_t vs = offsets[v], ve = offsets[v + 1];
-                const uint32_t p = lower_bound_u32(targets, vs, ve, u);
-                if (p == ve || targets[p] != u) bad = true;
-            }
-        }
-        if (__any_sync(kFullMask, bad)) {
-            if (lane == 0) atomicOr(asymmetric, 1u);
-            return;
-        }
-    }
+// Symmetry test: every entry u -> v needs v -> u; each entry binary-searches
+// u in the neighbour's list (entries taken in tiles, so hub lists are shared
+// by many blocks).
+__global__ void __launch_bounds__(256) csr_symmetry_kernel(const uint32_t* __restrict__ offsets,
+                                                           const uint32_t* __restrict__ targets, uint32_t V,
+                                                           uint32_t E, uint32_t* __restrict__ asymmetric) {
+    bool bad = false;
+    for_each_entry<256, 4>(offsets, V, E, [&](uint32_t j, uint32_t u) {
+        const uint32_t v = targets[j];
+        const uint32_t vs = offsets[v], ve = offsets[v + 1];
+        const uint32_t p = lower_bound_u32(targets, vs, ve, u);
+        if (p == ve || targets[p] != u) bad = true;
+    });
+    if (bad) atomicOr(asymmetric, 1u);
 }
 
 
@@ -133,10 +117,10 @@ Error graph_symmetry(GraphImpl& g, bool* symmetric) {
             DeviceBuffer<uint32_t> flag;
             GCU_TRY(flag.allocate(dev, 1));
             GCU_CUDA(cudaMemsetAsync(flag.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
-            unsigned blocks = static_cast<unsigned>(
-                std::min<uint64_t>(ceil_div_u64(g.num_nodes, 256), static_cast<uint64_t>(dev.sm_count) * 16));
+            unsigned blocks = static_cast<unsigned>(std::max<uint64_t>(
+                1, std::min<uint64_t>(ceil_div_u64(g.num_edges, 1024), static_cast<uint64_t>(dev.sm_count) * 16)));
             GCU_LAUNCH(dev, "csr_symmetry", csr_symmetry_kernel, blocks, 256, 0, g.offsets.ptr, g.targets.ptr,
-                       g.num_nodes, flag.ptr);
+                       g.num_nodes, g.num_edges, flag.ptr);
             uint32_t host = 0;
             GCU_CUDA(cudaMemcpyAsync(&host, flag.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
             GCU_TRY(dev.sync());
