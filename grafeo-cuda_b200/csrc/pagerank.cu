@@ -32,8 +32,10 @@
 //  * Row sums: FP32 Kahan sums per lane, FP64 across lanes (shuffle tree) and
 //    across segments. Epilogue per row v: r'[v] = (1-d)/N + d (sum +
 //    dangling/N); |r' - r| and the dangling mass of r' are summed as 64-bit
-//    fixed-point integers (2^-62 units) per CTA and reduced by the last block
-//    of the finishing kernel: integer sums do not depend on the order, so the
+//    fixed-point integers (2^-62 units) in registers per lane, then per warp
+//    and per CTA, and reduced by the last block of the finishing kernel (no
+//    shared-memory atomics: same-address atomics of a warp's rows cost a
+//    quarter of the L1TEX wavefronts); integer sums do not depend on the order, so the
 //    result is deterministic whatever the grid size (no float atomics);
 //    c'[v] = r'[v] / deg(v) is written for the next iteration.
 //  * The iteration loop stays on the device: each kernel reads a `done` flag
@@ -330,9 +332,9 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
     const uint2* __restrict__ units, double* __restrict__ seg_partial,
     unsigned long long* __restrict__ row_partials) {
     if (state->done) return;
-    // Loop invariants and the per-warp fixed-point sums live in shared memory,
-    // so that the unrolled gather loop keeps its 8 loads in flight within 32
-    // registers.
+    // Loop invariants live in shared memory, so that the unrolled gather loop
+    // keeps its 8 loads in flight within 32 registers; the fixed-point sums
+    // stay in registers per lane until the end.
     constexpr int kWarps = kPrThreads / 32;
     __shared__ double s_mass[2];                     // dangling mass, its uniform share
     __shared__ unsigned long long s_sum[2 * kWarps];  // per warp: L1 change, dangling mass of r'
@@ -345,6 +347,7 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
     __syncthreads();
     const uint32_t total_warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t first_unit = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    unsigned long long my_diff = 0, my_dangle = 0;
     {
         for (uint32_t b = first_unit; b < sched.total_blocks; b += total_warps) {
             uint32_t pi = 0;
@@ -425,8 +428,8 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
                         double d = 0.0, dg = 0.0;
                         pr_finish_row(row, v, re[q] - rs[q], rank_in, rank_out, contrib_out, outdeg, tele, base,
                                       damp, s_mass[1], s_mass[0], d, dg);
-                        atomicAdd(&s_sum[2 * warp], to_fixed(d));
-                        if (dg != 0.0) atomicAdd(&s_sum[2 * warp + 1], to_fixed(dg));
+                        my_diff += to_fixed(d);
+                        my_dangle += to_fixed(dg);
                     }
                 }
             } else {
@@ -436,11 +439,17 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
                     double d = 0.0, dg = 0.0;
                     pr_finish_row(row, 0.0, 0, rank_in, rank_out, contrib_out, outdeg, tele, base, damp, s_mass[1],
                                   s_mass[0], d, dg);
-                    atomicAdd(&s_sum[2 * warp], to_fixed(d));
-                    if (dg != 0.0) atomicAdd(&s_sum[2 * warp + 1], to_fixed(dg));
+                    my_diff += to_fixed(d);
+                    my_dangle += to_fixed(dg);
                 }
             }
         }
+    }
+    my_diff = warp_sum(my_diff);
+    my_dangle = warp_sum(my_dangle);
+    if (lane == 0) {
+        s_sum[2 * warp] = my_diff;
+        s_sum[2 * warp + 1] = my_dangle;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
