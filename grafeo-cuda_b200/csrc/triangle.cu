@@ -16,14 +16,20 @@
 //     entries u -> v, v > u, of |{w in N(u) ∩ N(v) : w > v}|
 //     (triangle_counting.cu:246-315), whatever the input.
 //  2. Counting: sum over DAG edges u -> v of |N+(u) ∩ N+(v)|, which counts
-//     every triangle exactly once. Vertex-centric: a warp hashes N+(u) into
-//     shared memory, then walks the wedges (v, w), v in N+(u), w in N+(v), 32 at
-//     a time with the (v, w) pairs balanced over the lanes by a warp scan of
-//     the d+(v), and probes each w in a shared-memory hash table of N+(u)
-//     (wedge.cuh). Vertices are bucketed by ceil(log2 d+); each bucket runs
-//     one of three variants (warp hash table up to 128 entries, CTA hash table
-//     up to 2048, CTA binary search beyond), by the fixed degree ranges or by
-//     an installed learned schedule (sched.cuh).
+//     every triangle exactly once. Each edge streams the shorter of the two
+//     lists against a shared-memory hash table of the longer one:
+//     - tail side (d+(v) <= d+(u)): a warp or CTA hashes N+(u), then walks
+//       the wedges (v, w), v in N+(u), w in N+(v), 32 at a time with the
+//       (v, w) pairs balanced over the lanes by a warp scan of the d+(v), and
+//       probes each w (wedge.cuh). Vertices are bucketed by ceil(log2 d+);
+//       each bucket runs one of three variants (warp hash table up to 128
+//       entries, CTA hash table up to 2048, CTA binary search beyond), by the
+//       fixed degree ranges or by an installed learned schedule (sched.cuh).
+//     - head side (2 <= d+(u) < d+(v)): the tails of such edges are gathered
+//       into in-lists of their heads; a warp or CTA hashes N+(v) and streams
+//       N+(u) for every tail u of a slice of v's in-list. On an R-MAT graph of
+//       scale 22 this cuts the probes from 2.9e10 (all edges tail side) to
+//       1.2e10.
 //  All indices are 64-bit where they can exceed 2^32, so there is no cap on the
 //  number of edges.
 #include <algorithm>
@@ -301,7 +307,7 @@ Error plan_buckets(DeviceImpl& dev, const uint32_t* d_offsets, uint32_t V, uint3
 // One launch of `variant` over bucket c's vertices; next = its handout counter (zeroed).
 template <class Sink>
 Error launch_bucket(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets, const BucketPlan& p, int c,
-                    int variant, uint32_t* next, Sink sink) {
+                    int variant, uint32_t* next, bool split, Sink sink) {
     const uint32_t n = p.host_counts[c];
     const uint32_t* list = p.list.ptr + p.host_starts[c];
     const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 8;
@@ -309,11 +315,147 @@ Error launch_bucket(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* 
         const unsigned grid = static_cast<unsigned>(
             std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(n, kWedgeWarps * kVertexBatch), cap)));
         GCU_LAUNCH(dev, "wedge_warp_bucket", wedge_warp_list_kernel<Sink>, grid, kWedgeThreads, 0, d_offsets,
-                   d_targets, list, n, next, sink);
+                   d_targets, list, n, next, split, sink);
     } else {
         const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(n, cap)));
         GCU_LAUNCH(dev, variant == 1 ? "wedge_cta_bucket" : "wedge_search_bucket", wedge_cta_list_kernel<Sink>, grid,
-                   kWedgeThreads, 0, d_offsets, d_targets, list, n, next, variant == 2 ? 1 : 0, sink);
+                   kWedgeThreads, 0, d_offsets, d_targets, list, n, next, variant == 2 ? 1 : 0, split, sink);
+    }
+    return ok();
+}
+
+// ---------------------------------------------------------------- head side
+
+// For every DAG entry u -> v with 2 <= d+(u) < d+(v): counts it for v (pass
+// without in_src) or places u in v's in-list (in_src given; counter zeroed).
+__global__ void __launch_bounds__(kOrientThreads) tc_head_lists_kernel(const uint32_t* __restrict__ offsets,
+                                                                       const uint32_t* __restrict__ targets,
+                                                                       uint32_t V, uint32_t m,
+                                                                       uint32_t* __restrict__ counter,
+                                                                       const uint32_t* __restrict__ in_off,
+                                                                       uint32_t* __restrict__ in_src) {
+    for_each_entry<kOrientThreads, kOrientItems>(offsets, V, m, [&](uint32_t j, uint32_t u) {
+        const uint32_t du = __ldg(offsets + u + 1) - __ldg(offsets + u);
+        if (du < 2) return;
+        const uint32_t v = ld_stream(targets + j);
+        const uint32_t dv = __ldg(offsets + v + 1) - __ldg(offsets + v);
+        if (du >= dv) return;
+        const uint32_t k = atomicAdd(counter + v, 1u);
+        if (in_src) in_src[in_off[v] + k] = u;
+    });
+}
+
+// Items of a head with `tails` tails in out-degree bucket c: warp items for
+// heads within a warp table, CTA items beyond.
+__host__ __device__ __forceinline__ uint32_t head_slices(int c, uint32_t tails) {
+    const uint32_t slice = bucket_fixed(c) == 0 ? kHeadWarpSlice : kHeadCtaSlice;
+    return static_cast<uint32_t>((static_cast<uint64_t>(tails) + slice - 1) / slice);
+}
+
+// Items per out-degree bucket of the heads (counts[c]); with `items`, also
+// writes every (v, slice) at cursor[c].
+__global__ void tc_head_items_kernel(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ in_off,
+                                     uint32_t V, uint32_t* __restrict__ counts, uint32_t* __restrict__ cursor,
+                                     uint2* __restrict__ items) {
+    __shared__ uint32_t s_count[kBuckets];
+    if (!items && threadIdx.x < kBuckets) s_count[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
+         v += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t tails = in_off[v + 1] - in_off[v];
+        if (tails == 0) continue;
+        const int c = bucket_of(offsets[v + 1] - offsets[v]);
+        const uint32_t n = head_slices(c, tails);
+        if (!items) {
+            atomicAdd(&s_count[c], n);
+        } else {
+            const uint32_t at = atomicAdd(cursor + c, n);
+            for (uint32_t k = 0; k < n; ++k) items[at + k] = make_uint2(static_cast<uint32_t>(v), k);
+        }
+    }
+    if (items) return;
+    __syncthreads();
+    if (threadIdx.x < kBuckets && s_count[threadIdx.x]) atomicAdd(counts + threadIdx.x, s_count[threadIdx.x]);
+}
+
+struct HeadPlan {
+    DeviceBuffer<uint32_t> in_off, in_src, counter, counts;
+    DeviceBuffer<uint2> items;
+    uint32_t host_counts[kBuckets] = {};
+    uint32_t host_starts[kBuckets] = {};
+};
+
+// In-lists of the head side and their (head, slice) items, bucketed by the
+// head's out-degree.
+Error plan_head(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets, uint32_t V, uint32_t m,
+                HeadPlan& h) {
+    GCU_TRY(h.counter.allocate(dev, static_cast<uint64_t>(V) + 1));
+    GCU_TRY(h.in_off.allocate(dev, static_cast<uint64_t>(V) + 1));
+    GCU_TRY(h.counts.allocate(dev, kBuckets));
+    GCU_CUDA(cudaMemsetAsync(h.counter.ptr, 0, sizeof(uint32_t) * (static_cast<uint64_t>(V) + 1), dev.stream),
+             "memset");
+    GCU_CUDA(cudaMemsetAsync(h.counts.ptr, 0, sizeof(uint32_t) * kBuckets, dev.stream), "memset");
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned tiles =
+        static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(m, kOrientTile), cap)));
+    const unsigned vgrid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(V, 256), cap)));
+    GCU_LAUNCH(dev, "tc_head_count", tc_head_lists_kernel, tiles, kOrientThreads, 0, d_offsets, d_targets, V, m,
+               h.counter.ptr, nullptr, nullptr);
+    GCU_TRY(exclusive_scan_u32(dev, h.counter.ptr, h.in_off.ptr, V));
+    GCU_LAUNCH(dev, "tc_head_items", tc_head_items_kernel, vgrid, 256, 0, d_offsets, h.in_off.ptr, V, h.counts.ptr,
+               nullptr, nullptr);
+    uint32_t tails = 0;
+    GCU_CUDA(cudaMemcpyAsync(&tails, h.in_off.ptr + V, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+    GCU_CUDA(cudaMemcpyAsync(h.host_counts, h.counts.ptr, sizeof(h.host_counts), cudaMemcpyDeviceToHost, dev.stream),
+             "copy");
+    GCU_TRY(dev.sync());
+    if (tails == 0) return ok();
+    // Buckets in descending order: the heaviest heads start first, and the
+    // items of each variant (c >= 12, 8..11, <= 7) are contiguous.
+    uint64_t total = 0;
+    for (int c = kBuckets - 1; c >= 0; --c) {
+        h.host_starts[c] = static_cast<uint32_t>(total);
+        total += h.host_counts[c];
+    }
+    GCU_TRY(h.in_src.allocate(dev, tails));
+    GCU_TRY(h.items.allocate(dev, std::max<uint64_t>(total, 1)));
+    GCU_CUDA(cudaMemsetAsync(h.counter.ptr, 0, sizeof(uint32_t) * (static_cast<uint64_t>(V) + 1), dev.stream),
+             "memset");
+    GCU_LAUNCH(dev, "tc_head_fill", tc_head_lists_kernel, tiles, kOrientThreads, 0, d_offsets, d_targets, V, m,
+               h.counter.ptr, h.in_off.ptr, h.in_src.ptr);
+    // The counts buffer becomes the item cursors.
+    GCU_CUDA(cudaMemcpyAsync(h.counts.ptr, h.host_starts, sizeof(h.host_starts), cudaMemcpyHostToDevice, dev.stream),
+             "copy");
+    GCU_LAUNCH(dev, "tc_head_items", tc_head_items_kernel, vgrid, 256, 0, d_offsets, h.in_off.ptr, V, nullptr,
+               h.counts.ptr, h.items.ptr);
+    return ok();
+}
+
+// Head-side items, one launch per variant over its contiguous buckets: CTA
+// binary search for heads beyond 2048 out-edges, CTA tables down to 129,
+// warp tables below.
+template <class Sink>
+Error launch_head(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets, const HeadPlan& h,
+                  uint32_t* next, Sink sink) {
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 8;
+    const int ranges[3][2] = {{kBuckets - 1, 12}, {11, 8}, {7, 0}};  // [hi, lo] buckets of variants 2, 1, 0
+    for (int r = 0; r < 3; ++r) {
+        const int hi = ranges[r][0], lo = ranges[r][1];
+        uint32_t n = 0;
+        for (int c = hi; c >= lo; --c) n += h.host_counts[c];
+        if (n == 0) continue;
+        const uint2* items = h.items.ptr + h.host_starts[hi];
+        const int variant = bucket_fixed(lo);
+        if (variant == 0) {
+            const unsigned grid = static_cast<unsigned>(
+                std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(n, kWedgeWarps * kVertexBatch), cap)));
+            GCU_LAUNCH(dev, "wedge_head_warp", wedge_head_warp_kernel<Sink>, grid, kWedgeThreads, 0, d_offsets,
+                       d_targets, items, n, h.in_off.ptr, h.in_src.ptr, next + r, sink);
+        } else {
+            const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(n, cap)));
+            GCU_LAUNCH(dev, "wedge_head_cta", wedge_head_cta_kernel<Sink>, grid, kWedgeThreads, 0, d_offsets,
+                       d_targets, items, n, h.in_off.ptr, h.in_src.ptr, next + r, variant == 2 ? 1 : 0, sink);
+        }
     }
     return ok();
 }
@@ -329,13 +471,19 @@ Error count_dag(GraphImpl& g, const uint32_t* d_offsets, const uint32_t* d_targe
     if (dev.schedule || trace) GCU_TRY(degree_stats(g, &stats));
     BucketPlan p;
     GCU_TRY(plan_buckets(dev, d_offsets, V, min_deg, m, stats, trace != nullptr, p));
+    HeadPlan head;
+    GCU_TRY(plan_head(dev, d_offsets, d_targets, V, m, head));
     const int runs = trace ? kSchedOut : 1;
-    DeviceBuffer<unsigned long long> totals;  // [bucket][variant] with trace, else [0]
-    DeviceBuffer<uint32_t> next;              // handout counters, same shape
-    GCU_TRY(totals.allocate(dev, kBuckets * runs));
-    GCU_TRY(next.allocate(dev, kBuckets * runs));
-    GCU_CUDA(cudaMemsetAsync(totals.ptr, 0, sizeof(unsigned long long) * kBuckets * runs, dev.stream), "memset");
-    GCU_CUDA(cudaMemsetAsync(next.ptr, 0, sizeof(uint32_t) * kBuckets * runs, dev.stream), "memset");
+    // [bucket][variant] with trace, else [0]; then the head side's total
+    // (slot kBuckets * runs with trace, else [0] too) and handout counters.
+    const int head_slot = trace ? kBuckets * runs : 0;
+    const int slots = kBuckets * runs + 1 + kBuckets;
+    DeviceBuffer<unsigned long long> totals;
+    DeviceBuffer<uint32_t> next;
+    GCU_TRY(totals.allocate(dev, slots));
+    GCU_TRY(next.allocate(dev, slots));
+    GCU_CUDA(cudaMemsetAsync(totals.ptr, 0, sizeof(unsigned long long) * slots, dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(next.ptr, 0, sizeof(uint32_t) * slots, dev.stream), "memset");
     std::vector<cudaEvent_t> ev;
     struct Events {
         std::vector<cudaEvent_t>& e;
@@ -354,19 +502,22 @@ Error count_dag(GraphImpl& g, const uint32_t* d_offsets, const uint32_t* d_targe
             int variant = bucket_fixed(c);
             const int pick = p.host_choices[c];
             if (pick >= 0 && ((valid >> pick) & 1u)) variant = pick;
-            GCU_TRY(launch_bucket(dev, d_offsets, d_targets, p, c, variant, next.ptr + c, CountSink{totals.ptr, 0}));
+            GCU_TRY(launch_bucket(dev, d_offsets, d_targets, p, c, variant, next.ptr + c, true,
+                                  CountSink{totals.ptr, 0}));
             continue;
         }
         for (int v = 0; v < kSchedOut; ++v) {
             if (!((valid >> v) & 1u)) continue;
             const int slot = c * kSchedOut + v;
             GCU_CUDA(cudaEventRecord(ev[2 * slot], dev.stream), "cudaEventRecord");
-            GCU_TRY(launch_bucket(dev, d_offsets, d_targets, p, c, v, next.ptr + slot,
+            GCU_TRY(launch_bucket(dev, d_offsets, d_targets, p, c, v, next.ptr + slot, true,
                                   CountSink{totals.ptr + slot, 0}));
             GCU_CUDA(cudaEventRecord(ev[2 * slot + 1], dev.stream), "cudaEventRecord");
         }
     }
-    std::vector<unsigned long long> host(kBuckets * runs);
+    GCU_TRY(launch_head(dev, d_offsets, d_targets, head, next.ptr + kBuckets * runs + 1,
+                        CountSink{totals.ptr + head_slot, 0}));
+    std::vector<unsigned long long> host(kBuckets * runs + 1);
     GCU_CUDA(cudaMemcpyAsync(host.data(), totals.ptr, sizeof(unsigned long long) * host.size(), cudaMemcpyDeviceToHost,
                              dev.stream),
              "copy");
@@ -375,7 +526,7 @@ Error count_dag(GraphImpl& g, const uint32_t* d_offsets, const uint32_t* d_targe
         *total = host[0];
         return ok();
     }
-    uint64_t sum = 0;
+    uint64_t sum = host[head_slot];
     trace->clear();
     for (int c = kBuckets - 1; c >= 0; --c) {
         if (p.host_counts[c] == 0) continue;
@@ -499,7 +650,7 @@ Error batch_tc_plan(GraphImpl& u, BatchTcPlan** out, std::string* tuning) {
                 if (!((valid >> v) & 1u)) continue;
                 GCU_CUDA(cudaEventRecord(ev[2 * v], dev.stream), "cudaEventRecord");
                 GCU_TRY(launch_bucket(dev, p->dag_offsets.ptr, p->dag_targets.ptr, p->buckets, c, v,
-                                      p->next.ptr + c * kSchedOut + v, VertexCountSink{scratch.ptr, 0}));
+                                      p->next.ptr + c * kSchedOut + v, false, VertexCountSink{scratch.ptr, 0}));
                 GCU_CUDA(cudaEventRecord(ev[2 * v + 1], dev.stream), "cudaEventRecord");
             }
             GCU_TRY(dev.sync());
@@ -534,7 +685,7 @@ Error batch_tc_launch(DeviceImpl& dev, BatchTcPlan& p, unsigned long long* per_v
     for (int c = kBuckets - 1; c >= 0; --c) {
         if (p.buckets.host_counts[c] == 0) continue;
         GCU_TRY(launch_bucket(dev, p.dag_offsets.ptr, p.dag_targets.ptr, p.buckets, c, p.variant[c], p.next.ptr + c,
-                              VertexCountSink{per_vertex, 0}));
+                              false, VertexCountSink{per_vertex, 0}));
     }
     return ok();
 }

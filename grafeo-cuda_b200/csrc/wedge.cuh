@@ -19,10 +19,13 @@ namespace gcu {
 constexpr uint32_t kEmptyKey = 0xFFFFFFFFu;
 constexpr uint32_t kNotFound = 0xFFFFFFFFu;
 
-// Smallest b >= 6 with 2^b >= 2n: a table of 2^b slots at load <= 1/2.
-__host__ __device__ __forceinline__ uint32_t table_bits(uint32_t n) {
+// Smallest b >= 6 with 2^b >= 4n, at most max_bits: a table of 2^b slots at
+// load <= 1/4 where the slots allow (most probes miss, and a miss walks the
+// run to the next empty slot: 1.4 slots on average at load 1/4, 2.5 at 1/2).
+// Callers keep n <= 2^(max_bits - 1), so the load never exceeds 1/2.
+__host__ __device__ __forceinline__ uint32_t table_bits(uint32_t n, uint32_t max_bits) {
     uint32_t b = 6;
-    while ((1u << b) < 2 * n) ++b;
+    while (b < max_bits && (1u << b) < 4 * n) ++b;
     return b;
 }
 
@@ -83,17 +86,20 @@ __device__ __forceinline__ uint32_t sorted_find(const uint32_t* a, uint32_t n, u
 // Walks the wedges of the out-neighbours v = list[c .. c + 31] of u (list =
 // N+(u), du entries); for every w in N+(v) that find(w) locates in N+(u) calls
 // hit(pos_v, pos_w, entry_vw): positions of v and w in N+(u) and the CSR entry
-// index of v -> w. s_excl / s_start are 32-word per-warp scratch.
+// index of v -> w. Out-neighbours with more than max_dv out-edges are skipped
+// (their edges are counted from the other end). s_excl / s_start are 32-word
+// per-warp scratch.
 template <class Find, class Hit>
 __device__ __forceinline__ void wedge_chunk(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
                                             const uint32_t* list, uint32_t du, uint32_t c, uint32_t* s_excl,
-                                            uint32_t* s_start, Find find, Hit hit) {
+                                            uint32_t* s_start, uint32_t max_dv, Find find, Hit hit) {
     const unsigned lane = lane_id();
     uint32_t vs = 0, dv = 0;
     if (c + lane < du) {
         const uint32_t v = list[c + lane];
         vs = offsets[v];
         dv = offsets[v + 1] - vs;
+        if (dv > max_dv) dv = 0;
     }
     const uint32_t inc = warp_inclusive_scan(dv);
     const uint32_t total = __shfl_sync(kFullMask, inc, 31);
@@ -101,15 +107,12 @@ __device__ __forceinline__ void wedge_chunk(const uint32_t* __restrict__ offsets
     s_excl[lane] = inc - dv;
     s_start[lane] = vs;
     __syncwarp();
+    // lo = the largest j with s_excl[j] <= k (the v owning wedge k); k only
+    // grows, so each lane walks forward from its last v instead of searching
+    // (one shared-memory read per wedge on long lists instead of five).
+    uint32_t lo = 0;
     for (uint32_t k = lane; k < total; k += 32) {
-        uint32_t lo = 0, hi = 32;  // largest j with s_excl[j] <= k (the v owning wedge k)
-        while (hi - lo > 1) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (s_excl[mid] <= k)
-                lo = mid;
-            else
-                hi = mid;
-        }
+        while (lo < 31 && s_excl[lo + 1] <= k) ++lo;
         const uint32_t entry = s_start[lo] + (k - s_excl[lo]);
         const uint32_t p = find(targets[entry]);
         if (p != kNotFound) hit(c + lo, p, entry);
@@ -121,9 +124,11 @@ __device__ __forceinline__ void wedge_chunk(const uint32_t* __restrict__ offsets
 constexpr int kWedgeThreads = 256;
 constexpr int kWedgeWarps = kWedgeThreads / 32;
 constexpr uint32_t kWarpMaxDeg = 128;   // warp kernel: out-lists up to this length
-constexpr uint32_t kWarpSlots = 256;    // hash slots per warp (load <= 1/2)
+constexpr uint32_t kWarpBits = 8;
+constexpr uint32_t kWarpSlots = 1u << kWarpBits;  // hash slots per warp (load <= 1/2)
 constexpr uint32_t kCtaMaxDeg = 2048;   // CTA kernel: hash table up to this length
-constexpr uint32_t kCtaSlots = 4096;
+constexpr uint32_t kCtaBits = 12;
+constexpr uint32_t kCtaSlots = 1u << kCtaBits;
 constexpr uint32_t kVertexBatch = 8;    // vertices fetched per warp at a time
 
 // A Sink receives every triangle: hit(row_base, pos_v, pos_w, entry_vw) with
@@ -155,7 +160,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_warp_kernel(const uint32_
         for (uint32_t u = base; u < last; ++u) {
             const uint32_t s = offsets[u], du = offsets[u + 1] - s;
             if (du < min_deg || du > kWarpMaxDeg) continue;
-            const uint32_t bits = table_bits(du);
+            const uint32_t bits = table_bits(du, kWarpBits);
             __syncwarp();
             for (uint32_t k = lane; k < (1u << bits); k += 32) keys[k] = kEmptyKey;
             __syncwarp();
@@ -163,7 +168,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_warp_kernel(const uint32_
             __syncwarp();
             for (uint32_t c = 0; c < du; c += 32)
                 wedge_chunk(
-                    offsets, targets, targets + s, du, c, s_excl[warp], s_start[warp],
+                    offsets, targets, targets + s, du, c, s_excl[warp], s_start[warp], 0xFFFFFFFFu,
                     [&](uint32_t w) { return hash_find<kPos>(keys, pos, bits, w); },
                     [&](uint32_t pv, uint32_t pw, uint32_t evw) { sink.hit(s, pv, pw, evw); });
         }
@@ -207,7 +212,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_kernel(const uint32_t
         const uint32_t s = offsets[u], du = offsets[u + 1] - s;
         const uint32_t* list = targets + s;
         const bool use_table = du <= kCtaMaxDeg;
-        const uint32_t bits = use_table ? table_bits(du) : 0;
+        const uint32_t bits = use_table ? table_bits(du, kCtaBits) : 0;
         if (use_table) {
             for (uint32_t k = threadIdx.x; k < (1u << bits); k += kWedgeThreads) s_keys[k] = kEmptyKey;
             __syncthreads();
@@ -216,7 +221,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_kernel(const uint32_t
         }
         for (uint32_t c = warp * 32; c < du; c += kWedgeThreads)
             wedge_chunk(
-                offsets, targets, list, du, c, s_excl[warp], s_start[warp],
+                offsets, targets, list, du, c, s_excl[warp], s_start[warp], 0xFFFFFFFFu,
                 [&](uint32_t w) {
                     return use_table ? hash_find<kPos>(s_keys, pos, bits, w) : sorted_find(list, du, w);
                 },
@@ -230,7 +235,10 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_kernel(const uint32_t
 // The same intersections over an explicit vertex list (one out-degree bucket
 // of a DAG), so that a schedule can pick the variant per bucket. Their sinks
 // also get end_vertex(u) from every warp that worked on u, once it is done
-// with u (all 32 lanes call it).
+// with u (all 32 lanes call it). With `split`, an edge u -> v whose head has
+// more out-edges than its tail (d+(v) > d+(u) >= 2) is left to the head-side
+// kernels below, which stream the shorter list N+(u) against a table of
+// N+(v): every edge then costs min(d+(u), d+(v)) probes instead of d+(v).
 
 // Warp per listed vertex; a shared hash table per warp for out-lists of at
 // most kWarpMaxDeg entries, binary search in global memory beyond (the
@@ -240,7 +248,8 @@ template <class Sink>
 __global__ void __launch_bounds__(kWedgeThreads) wedge_warp_list_kernel(const uint32_t* __restrict__ offsets,
                                                                         const uint32_t* __restrict__ targets,
                                                                         const uint32_t* __restrict__ list, uint32_t n,
-                                                                        uint32_t* __restrict__ next, Sink sink) {
+                                                                        uint32_t* __restrict__ next, bool split,
+                                                                        Sink sink) {
     constexpr bool kPos = Sink::kNeedsPos;
     __shared__ uint32_t s_keys[kWedgeWarps][kWarpSlots];
     __shared__ uint32_t s_pos[kPos ? kWedgeWarps : 1][kPos ? kWarpSlots : 1];
@@ -259,7 +268,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_warp_list_kernel(const ui
             const uint32_t u = list[h];
             const uint32_t s = offsets[u], du = offsets[u + 1] - s;
             const bool use_table = du <= kWarpMaxDeg;
-            const uint32_t bits = use_table ? table_bits(du) : 0;
+            const uint32_t bits = use_table ? table_bits(du, kWarpBits) : 0;
             __syncwarp();
             if (use_table) {
                 for (uint32_t k = lane; k < (1u << bits); k += 32) keys[k] = kEmptyKey;
@@ -268,9 +277,10 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_warp_list_kernel(const ui
                 __syncwarp();
             }
             const uint32_t* ulist = targets + s;
+            const uint32_t max_dv = split && du >= 2 ? du : 0xFFFFFFFFu;
             for (uint32_t c = 0; c < du; c += 32)
                 wedge_chunk(
-                    offsets, targets, ulist, du, c, s_excl[warp], s_start[warp],
+                    offsets, targets, ulist, du, c, s_excl[warp], s_start[warp], max_dv,
                     [&](uint32_t w) {
                         return use_table ? hash_find<kPos>(keys, pos, bits, w) : sorted_find(ulist, du, w);
                     },
@@ -289,7 +299,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_list_kernel(const uin
                                                                        const uint32_t* __restrict__ targets,
                                                                        const uint32_t* __restrict__ list, uint32_t n,
                                                                        uint32_t* __restrict__ next, int search,
-                                                                       Sink sink) {
+                                                                       bool split, Sink sink) {
     constexpr bool kPos = Sink::kNeedsPos;
     __shared__ uint32_t s_keys[kCtaSlots];
     __shared__ uint32_t s_pos[kPos ? kCtaSlots : 1];
@@ -307,22 +317,131 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_list_kernel(const uin
         const uint32_t s = offsets[u], du = offsets[u + 1] - s;
         const uint32_t* ulist = targets + s;
         const bool use_table = !search && du <= kCtaMaxDeg;
-        const uint32_t bits = use_table ? table_bits(du) : 0;
+        const uint32_t bits = use_table ? table_bits(du, kCtaBits) : 0;
         if (use_table) {
             for (uint32_t k = threadIdx.x; k < (1u << bits); k += kWedgeThreads) s_keys[k] = kEmptyKey;
             __syncthreads();
             for (uint32_t k = threadIdx.x; k < du; k += kWedgeThreads) hash_insert<kPos>(s_keys, pos, bits, ulist[k], k);
             __syncthreads();
         }
+        const uint32_t max_dv = split && du >= 2 ? du : 0xFFFFFFFFu;
         for (uint32_t c = warp * 32; c < du; c += kWedgeThreads)
             wedge_chunk(
-                offsets, targets, ulist, du, c, s_excl[warp], s_start[warp],
+                offsets, targets, ulist, du, c, s_excl[warp], s_start[warp], max_dv,
                 [&](uint32_t w) {
                     return use_table ? hash_find<kPos>(s_keys, pos, bits, w) : sorted_find(ulist, du, w);
                 },
                 [&](uint32_t pv, uint32_t pw, uint32_t evw) { sink.hit(s, pv, pw, evw); });
         sink.end_vertex(u);
         __syncthreads();  // the table and s_item are reused by the next list
+    }
+    sink.finish();
+}
+
+// ---------------------------------------------------------------- head-side kernels
+// Item (v, k): the k-th slice of `slice` tails of v's in-list (in_src from
+// in_off[v], the tails u with 2 <= d+(u) < d+(v)); slices are short enough
+// that no single item holds up the end of a launch. The table holds N+(v);
+// the out-lists of the slice's tails are streamed against it, balanced over
+// the lanes by wedge_chunk; a hit w is a triangle u -> v, u -> w, v -> w.
+// Sinks only count (hit positions are not the tail's).
+constexpr uint32_t kHeadWarpSlice = 256;   // tails per item of the warp kernel
+constexpr uint32_t kHeadCtaSlice = 1024;   // tails per item of the CTA kernel
+
+__device__ __forceinline__ void head_slice(const uint2 item, const uint32_t* __restrict__ in_off,
+                                           const uint32_t* __restrict__ in_src, uint32_t slice,
+                                           const uint32_t*& tails, uint32_t& count) {
+    const uint32_t b = in_off[item.x] + item.y * slice, e = in_off[item.x + 1];
+    tails = in_src + b;
+    count = min(slice, e - b);
+}
+
+// Warp per item, heads with at most kWarpMaxDeg out-edges (binary search of
+// N+(v) beyond, to stay in bounds whatever the items hold).
+template <class Sink>
+__global__ void __launch_bounds__(kWedgeThreads) wedge_head_warp_kernel(
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, const uint2* __restrict__ items,
+    uint32_t n, const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ in_src, uint32_t* __restrict__ next,
+    Sink sink) {
+    __shared__ uint32_t s_keys[kWedgeWarps][kWarpSlots];
+    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_start[kWedgeWarps][32];
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    uint32_t* keys = s_keys[warp];
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(next, kVertexBatch);
+        base = __shfl_sync(kFullMask, base, 0);
+        if (base >= n) break;
+        const uint32_t last = min(base + kVertexBatch, n);
+        for (uint32_t h = base; h < last; ++h) {
+            const uint2 item = items[h];
+            const uint32_t s = offsets[item.x], dv = offsets[item.x + 1] - s;
+            const uint32_t* vlist = targets + s;
+            const bool use_table = dv <= kWarpMaxDeg;
+            const uint32_t bits = use_table ? table_bits(dv, kWarpBits) : 0;
+            __syncwarp();
+            if (use_table) {
+                for (uint32_t k = lane; k < (1u << bits); k += 32) keys[k] = kEmptyKey;
+                __syncwarp();
+                for (uint32_t k = lane; k < dv; k += 32) hash_insert<false>(keys, nullptr, bits, vlist[k], k);
+                __syncwarp();
+            }
+            const uint32_t* tails;
+            uint32_t count;
+            head_slice(item, in_off, in_src, kHeadWarpSlice, tails, count);
+            for (uint32_t c = 0; c < count; c += 32)
+                wedge_chunk(
+                    offsets, targets, tails, count, c, s_excl[warp], s_start[warp], 0xFFFFFFFFu,
+                    [&](uint32_t w) {
+                        return use_table ? hash_find<false>(keys, nullptr, bits, w) : sorted_find(vlist, dv, w);
+                    },
+                    [&](uint32_t pu, uint32_t pw, uint32_t e) { sink.hit(s, pu, pw, e); });
+        }
+    }
+    sink.finish();
+}
+
+// CTA per item: a shared table of N+(v) (at most kCtaMaxDeg entries, unless
+// `search`) or binary search of N+(v) in global memory.
+template <class Sink>
+__global__ void __launch_bounds__(kWedgeThreads) wedge_head_cta_kernel(
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, const uint2* __restrict__ items,
+    uint32_t n, const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ in_src, uint32_t* __restrict__ next,
+    int search, Sink sink) {
+    __shared__ uint32_t s_keys[kCtaSlots];
+    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_start[kWedgeWarps][32];
+    __shared__ uint32_t s_item;
+    const unsigned warp = threadIdx.x >> 5;
+    while (true) {
+        if (threadIdx.x == 0) s_item = atomicAdd(next, 1u);
+        __syncthreads();
+        const uint32_t h = s_item;
+        if (h >= n) break;
+        const uint2 item = items[h];
+        const uint32_t s = offsets[item.x], dv = offsets[item.x + 1] - s;
+        const uint32_t* vlist = targets + s;
+        const bool use_table = !search && dv <= kCtaMaxDeg;
+        const uint32_t bits = use_table ? table_bits(dv, kCtaBits) : 0;
+        if (use_table) {
+            for (uint32_t k = threadIdx.x; k < (1u << bits); k += kWedgeThreads) s_keys[k] = kEmptyKey;
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < dv; k += kWedgeThreads)
+                hash_insert<false>(s_keys, nullptr, bits, vlist[k], k);
+            __syncthreads();
+        }
+        const uint32_t* tails;
+        uint32_t count;
+        head_slice(item, in_off, in_src, kHeadCtaSlice, tails, count);
+        for (uint32_t c = warp * 32; c < count; c += kWedgeThreads)
+            wedge_chunk(
+                offsets, targets, tails, count, c, s_excl[warp], s_start[warp], 0xFFFFFFFFu,
+                [&](uint32_t w) {
+                    return use_table ? hash_find<false>(s_keys, nullptr, bits, w) : sorted_find(vlist, dv, w);
+                },
+                [&](uint32_t pu, uint32_t pw, uint32_t e) { sink.hit(s, pu, pw, e); });
+        __syncthreads();  // the table and s_item are reused by the next item
     }
     sink.finish();
 }
