@@ -87,8 +87,8 @@ __device__ __forceinline__ uint32_t sorted_find(const uint32_t* a, uint32_t n, u
 // N+(u), du entries); for every w in N+(v) that find(w) locates in N+(u) calls
 // hit(pos_v, pos_w, entry_vw): positions of v and w in N+(u) and the CSR entry
 // index of v -> w. Out-neighbours with more than max_dv out-edges are skipped
-// (their edges are counted from the other end). s_excl / s_start are 32-word
-// per-warp scratch.
+// (their edges are counted from the other end). s_excl (33 words) / s_start
+// (32 words) are per-warp scratch.
 template <class Find, class Hit>
 __device__ __forceinline__ void wedge_chunk(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
                                             const uint32_t* list, uint32_t du, uint32_t c, uint32_t* s_excl,
@@ -106,17 +106,33 @@ __device__ __forceinline__ void wedge_chunk(const uint32_t* __restrict__ offsets
     __syncwarp();
     s_excl[lane] = inc - dv;
     s_start[lane] = vs;
+    if (lane == 0) s_excl[32] = 0xFFFFFFFFu;  // stops the walk
     __syncwarp();
     // lo = the largest j with s_excl[j] <= k (the v owning wedge k); k only
-    // grows, so each lane walks forward from its last v instead of searching
-    // (one shared-memory read per wedge on long lists instead of five).
-    uint32_t lo = 0;
+    // grows, so each lane walks forward from its last v, with that v's first
+    // wedge, list start and the next v's first wedge kept in registers: no
+    // shared-memory read per wedge while a lane stays on one v.
+    uint32_t lo = 0, first = 0, start = s_start[0], next = s_excl[1];
     for (uint32_t k = lane; k < total; k += 32) {
-        while (lo < 31 && s_excl[lo + 1] <= k) ++lo;
-        const uint32_t entry = s_start[lo] + (k - s_excl[lo]);
+        while (next <= k) {
+            ++lo;
+            first = next;
+            start = s_start[lo];
+            next = s_excl[lo + 1];
+        }
+        const uint32_t entry = start + (k - first);
         const uint32_t p = find(targets[entry]);
         if (p != kNotFound) hit(c + lo, p, entry);
     }
+}
+
+// First list entry of the next 32-entry chunk of the current CTA item
+// (shared counter reset with the item): the warps of a CTA take chunks as
+// they finish, so one long chunk does not keep the others at the barrier.
+__device__ __forceinline__ uint32_t next_chunk(uint32_t* s_chunk) {
+    uint32_t c = 0;
+    if (lane_id() == 0) c = atomicAdd(s_chunk, 32u);
+    return __shfl_sync(kFullMask, c, 0);
 }
 
 // ---------------------------------------------------------------- kernels
@@ -146,7 +162,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_warp_kernel(const uint32_
     constexpr bool kPos = Sink::kNeedsPos;
     __shared__ uint32_t s_keys[kWedgeWarps][kWarpSlots];
     __shared__ uint32_t s_pos[kPos ? kWedgeWarps : 1][kPos ? kWarpSlots : 1];
-    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_excl[kWedgeWarps][33];
     __shared__ uint32_t s_start[kWedgeWarps][32];
     const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
     uint32_t* keys = s_keys[warp];
@@ -197,14 +213,17 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_kernel(const uint32_t
     constexpr bool kPos = Sink::kNeedsPos;
     __shared__ uint32_t s_keys[kCtaSlots];
     __shared__ uint32_t s_pos[kPos ? kCtaSlots : 1];
-    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_excl[kWedgeWarps][33];
     __shared__ uint32_t s_start[kWedgeWarps][32];
-    __shared__ uint32_t s_item;
+    __shared__ uint32_t s_item, s_chunk;
     const unsigned warp = threadIdx.x >> 5;
     const uint32_t n = *long_count;
     uint32_t* pos = kPos ? s_pos : nullptr;
     while (true) {
-        if (threadIdx.x == 0) s_item = atomicAdd(next_item, 1u);
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(next_item, 1u);
+            s_chunk = 0;
+        }
         __syncthreads();
         const uint32_t h = s_item;
         if (h >= n) break;
@@ -219,7 +238,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_kernel(const uint32_t
             for (uint32_t k = threadIdx.x; k < du; k += kWedgeThreads) hash_insert<kPos>(s_keys, pos, bits, list[k], k);
             __syncthreads();
         }
-        for (uint32_t c = warp * 32; c < du; c += kWedgeThreads)
+        for (uint32_t c = next_chunk(&s_chunk); c < du; c = next_chunk(&s_chunk))
             wedge_chunk(
                 offsets, targets, list, du, c, s_excl[warp], s_start[warp], 0xFFFFFFFFu,
                 [&](uint32_t w) {
@@ -253,7 +272,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_warp_list_kernel(const ui
     constexpr bool kPos = Sink::kNeedsPos;
     __shared__ uint32_t s_keys[kWedgeWarps][kWarpSlots];
     __shared__ uint32_t s_pos[kPos ? kWedgeWarps : 1][kPos ? kWarpSlots : 1];
-    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_excl[kWedgeWarps][33];
     __shared__ uint32_t s_start[kWedgeWarps][32];
     const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
     uint32_t* keys = s_keys[warp];
@@ -303,13 +322,16 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_list_kernel(const uin
     constexpr bool kPos = Sink::kNeedsPos;
     __shared__ uint32_t s_keys[kCtaSlots];
     __shared__ uint32_t s_pos[kPos ? kCtaSlots : 1];
-    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_excl[kWedgeWarps][33];
     __shared__ uint32_t s_start[kWedgeWarps][32];
-    __shared__ uint32_t s_item;
+    __shared__ uint32_t s_item, s_chunk;
     const unsigned warp = threadIdx.x >> 5;
     uint32_t* pos = kPos ? s_pos : nullptr;
     while (true) {
-        if (threadIdx.x == 0) s_item = atomicAdd(next, 1u);
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(next, 1u);
+            s_chunk = 0;
+        }
         __syncthreads();
         const uint32_t h = s_item;
         if (h >= n) break;
@@ -325,7 +347,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_list_kernel(const uin
             __syncthreads();
         }
         const uint32_t max_dv = split && du >= 2 ? du : 0xFFFFFFFFu;
-        for (uint32_t c = warp * 32; c < du; c += kWedgeThreads)
+        for (uint32_t c = next_chunk(&s_chunk); c < du; c = next_chunk(&s_chunk))
             wedge_chunk(
                 offsets, targets, ulist, du, c, s_excl[warp], s_start[warp], max_dv,
                 [&](uint32_t w) {
@@ -364,7 +386,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_head_warp_kernel(
     uint32_t n, const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ in_src, uint32_t* __restrict__ next,
     Sink sink) {
     __shared__ uint32_t s_keys[kWedgeWarps][kWarpSlots];
-    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_excl[kWedgeWarps][33];
     __shared__ uint32_t s_start[kWedgeWarps][32];
     const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
     uint32_t* keys = s_keys[warp];
@@ -410,12 +432,15 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_head_cta_kernel(
     uint32_t n, const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ in_src, uint32_t* __restrict__ next,
     int search, Sink sink) {
     __shared__ uint32_t s_keys[kCtaSlots];
-    __shared__ uint32_t s_excl[kWedgeWarps][32];
+    __shared__ uint32_t s_excl[kWedgeWarps][33];
     __shared__ uint32_t s_start[kWedgeWarps][32];
-    __shared__ uint32_t s_item;
+    __shared__ uint32_t s_item, s_chunk;
     const unsigned warp = threadIdx.x >> 5;
     while (true) {
-        if (threadIdx.x == 0) s_item = atomicAdd(next, 1u);
+        if (threadIdx.x == 0) {
+            s_item = atomicAdd(next, 1u);
+            s_chunk = 0;
+        }
         __syncthreads();
         const uint32_t h = s_item;
         if (h >= n) break;
@@ -434,7 +459,7 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_head_cta_kernel(
         const uint32_t* tails;
         uint32_t count;
         head_slice(item, in_off, in_src, kHeadCtaSlice, tails, count);
-        for (uint32_t c = warp * 32; c < count; c += kWedgeThreads)
+        for (uint32_t c = next_chunk(&s_chunk); c < count; c = next_chunk(&s_chunk))
             wedge_chunk(
                 offsets, targets, tails, count, c, s_excl[warp], s_start[warp], 0xFFFFFFFFu,
                 [&](uint32_t w) {
