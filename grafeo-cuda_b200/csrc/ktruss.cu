@@ -214,43 +214,209 @@ __global__ void kt_round_filter_kernel(const uint32_t* __restrict__ targets, con
 // alive at the start of the round is destroyed: each of its edges that
 // survives the round loses one support. A triangle with several edges removed
 // in this round is handled once, by the removed edge with the smallest id.
-__global__ void __launch_bounds__(256) kt_peel_kernel(const uint32_t* __restrict__ offsets,
+// With `next`, an edge whose support falls from `threshold` to below it is
+// listed there: supports only fall by one at a time, so every surviving edge
+// that the next round removes is listed exactly once, and that round needs no
+// scan of the alive edges.
+//
+// The shorter of the two lists is walked (the longer one binary-searched) in
+// chunks of kPeelChunk entries, one warp per chunk, so that a round that
+// removes a few hub edges spreads their lists over the whole GPU instead of
+// waiting on one warp per edge.
+constexpr uint32_t kPeelChunk = 256;
+
+struct PeelEdge {
+    uint32_t a, b;       // the removed edge
+    uint32_t x, y;       // the walked end and the searched end
+    uint32_t xs, xe, ys, ye;
+};
+
+// Lists of the live CSR `lv` (the graph's CSR, or its alive entries after a
+// compaction); e is an entry of the graph's CSR.
+struct LiveCsr {
+    const uint32_t* offsets;
+    const uint32_t* targets;
+    const uint32_t* eid;  // graph entry of each live entry (nullptr: the graph's CSR itself)
+    __device__ __forceinline__ uint32_t entry(uint32_t p) const { return eid ? eid[p] : p; }
+};
+
+__device__ __forceinline__ PeelEdge peel_edge(const LiveCsr& lv, const uint32_t* __restrict__ targets,
+                                              const uint32_t* __restrict__ src, uint32_t e) {
+    const uint32_t* __restrict__ offsets = lv.offsets;
+    PeelEdge p;
+    p.a = src[e];
+    p.b = targets[e];
+    p.xs = offsets[p.a];
+    p.xe = offsets[p.a + 1];
+    p.ys = offsets[p.b];
+    p.ye = offsets[p.b + 1];
+    p.x = p.a;
+    p.y = p.b;
+    if (p.xe - p.xs > p.ye - p.ys) {
+        uint32_t t = p.xs; p.xs = p.ys; p.ys = t;
+        t = p.xe; p.xe = p.ye; p.ye = t;
+        p.x = p.b;
+        p.y = p.a;
+    }
+    return p;
+}
+
+// chunks[i] = the walk chunks of removed edge i (at least one).
+__global__ void kt_peel_chunks_kernel(const LiveCsr lv, const uint32_t* __restrict__ targets,
+                                      const uint32_t* __restrict__ src, const uint32_t* __restrict__ removed,
+                                      const uint32_t* __restrict__ removed_count, uint32_t* __restrict__ chunks) {
+    const uint32_t n = *removed_count;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const PeelEdge p = peel_edge(lv, targets, src, removed[i]);
+        chunks[i] = max(1u, (p.xe - p.xs + kPeelChunk - 1) / kPeelChunk);
+    }
+}
+
+// Warp per chunk: chunk_start (n + 1 words) is the exclusive scan of the
+// chunk counts; each warp finds its edge by a binary search of it.
+__global__ void __launch_bounds__(256) kt_peel_kernel(const LiveCsr lv,
                                                       const uint32_t* __restrict__ targets,
                                                       const uint32_t* __restrict__ src,
                                                       const uint32_t* __restrict__ rev,
                                                       const uint32_t* __restrict__ state,
                                                       uint32_t* __restrict__ support,
                                                       const uint32_t* __restrict__ removed,
-                                                      const uint32_t* __restrict__ removed_count, uint32_t round) {
+                                                      const uint32_t* __restrict__ removed_count,
+                                                      const uint32_t* __restrict__ chunk_start, uint32_t round,
+                                                      uint32_t threshold, uint32_t* __restrict__ next,
+                                                      uint32_t* __restrict__ next_count) {
     const unsigned lane = lane_id();
     const uint32_t n = *removed_count;
+    const uint32_t total = chunk_start[n];
     const uint64_t nwarps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
-    for (uint64_t i = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
-        const uint32_t e = removed[i];
-        const uint32_t a = src[e], b = targets[e];
-        uint32_t xs = offsets[a], xe = offsets[a + 1], ys = offsets[b], ye = offsets[b + 1];
-        uint32_t x = a, y = b;
-        if (xe - xs > ye - ys) {  // walk the shorter list, search the longer
-            uint32_t t = xs; xs = ys; ys = t;
-            t = xe; xe = ye; ye = t;
-            x = b;
-            y = a;
+    for (uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; w < total; w += nwarps) {
+        // i = the largest index with chunk_start[i] <= w (every edge has a chunk).
+        uint32_t lo = 0, hi = n;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (chunk_start[mid] <= w)
+                lo = mid;
+            else
+                hi = mid;
         }
-        for (uint32_t p = xs + lane; p < xe; p += 32) {
-            const uint32_t w = targets[p];
-            if (w == a || w == b) continue;
-            const uint32_t e1 = x < w ? p : rev[p];
+        const uint32_t e = removed[lo];
+        const PeelEdge pe = peel_edge(lv, targets, src, e);
+        const uint32_t begin = pe.xs + (static_cast<uint32_t>(w) - chunk_start[lo]) * kPeelChunk;
+        const uint32_t end = min(begin + kPeelChunk, pe.xe);
+        for (uint32_t p = begin + lane; p < end; p += 32) {
+            const uint32_t wv = lv.targets[p];
+            if (wv == pe.a || wv == pe.b) continue;
+            const uint32_t j1 = lv.entry(p);
+            const uint32_t e1 = pe.x < wv ? j1 : rev[j1];
             const uint32_t s1 = state[e1];
             if (s1 != 0 && s1 != round) continue;
-            const uint32_t q = lower_bound_u32(targets, ys, ye, w);
-            if (q == ye || targets[q] != w) continue;
-            const uint32_t e2 = y < w ? q : rev[q];
+            const uint32_t q = lower_bound_u32(lv.targets, pe.ys, pe.ye, wv);
+            if (q == pe.ye || lv.targets[q] != wv) continue;
+            const uint32_t j2 = lv.entry(q);
+            const uint32_t e2 = pe.y < wv ? j2 : rev[j2];
             const uint32_t s2 = state[e2];
             if (s2 != 0 && s2 != round) continue;
             if ((s1 == round && e1 < e) || (s2 == round && e2 < e)) continue;
-            if (s1 == 0) atomicSub(support + e1, 1u);
-            if (s2 == 0) atomicSub(support + e2, 1u);
+            if (s1 == 0 && atomicSub(support + e1, 1u) == threshold && next) next[atomicAdd(next_count, 1u)] = e1;
+            if (s2 == 0 && atomicSub(support + e2, 1u) == threshold && next) next[atomicAdd(next_count, 1u)] = e2;
         }
+    }
+}
+
+// One peel: chunk counts of the n removed edges, their scan, the chunk walk.
+// chunks holds n + 1 words.
+static Error launch_peel(DeviceImpl& dev, GraphImpl& g, const LiveCsr& lv, const uint32_t* src,
+                         const uint32_t* rev, const uint32_t* state, uint32_t* support, const uint32_t* list,
+                         const uint32_t* count, uint32_t n, uint32_t* chunks, uint32_t round, uint32_t threshold,
+                         uint32_t* next, uint32_t* next_count) {
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(n, 256), cap)));
+    GCU_LAUNCH(dev, "kt_peel_chunks", kt_peel_chunks_kernel, grid, 256, 0, lv, g.targets.ptr, src, list, count,
+               chunks);
+    GCU_TRY(exclusive_scan_u32(dev, chunks, chunks, n));
+    GCU_LAUNCH(dev, "kt_peel", kt_peel_kernel, static_cast<unsigned>(cap), 256, 0, lv, g.targets.ptr, src, rev,
+               state, support, list, count, chunks, round, threshold, next, next_count);
+    return ok();
+}
+
+// ---------------------------------------------------------------- live CSR compaction
+
+// keep[p] for every live entry p = u -> w: not a self-loop and its edge alive.
+__global__ void __launch_bounds__(256) kt_live_flag_kernel(const LiveCsr lv, uint32_t V, uint32_t L,
+                                                           const uint32_t* __restrict__ rev,
+                                                           const uint32_t* __restrict__ state,
+                                                           uint32_t* __restrict__ keep) {
+    for_each_entry<256, 4>(lv.offsets, V, L, [&](uint32_t p, uint32_t u) {
+        const uint32_t w = lv.targets[p];
+        const uint32_t j = lv.entry(p);
+        keep[p] = (u != w && state[u < w ? j : rev[j]] == 0) ? 1u : 0u;
+    });
+}
+
+__global__ void kt_live_offsets_kernel(const uint32_t* __restrict__ offsets, uint32_t V,
+                                       const uint32_t* __restrict__ pos, uint32_t* __restrict__ out) {
+    for (uint64_t u = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; u <= V;
+         u += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        out[u] = pos[offsets[u]];
+}
+
+__global__ void kt_live_fill_kernel(const LiveCsr lv, uint32_t L, const uint32_t* __restrict__ pos,
+                                    uint32_t* __restrict__ targets, uint32_t* __restrict__ eid) {
+    for (uint64_t p = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < L;
+         p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t at = pos[p];
+        if (pos[p + 1] == at) continue;
+        targets[at] = lv.targets[p];
+        eid[at] = lv.entry(p);
+    }
+}
+
+// The alive entries of `lv` (L entries) in a new CSR (same order), so that
+// the peel of later rounds walks alive lists only.
+struct LiveBuffers {
+    DeviceBuffer<uint32_t> offsets, targets, eid;
+    uint32_t entries = 0;
+};
+
+static Error compact_live(DeviceImpl& dev, uint32_t V, const LiveCsr& lv, uint32_t L, const uint32_t* rev,
+                          const uint32_t* state, LiveBuffers* out) {
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    DeviceBuffer<uint32_t> pos;
+    GCU_TRY(pos.allocate(dev, static_cast<uint64_t>(L) + 1));
+    GCU_TRY(out->offsets.allocate(dev, static_cast<uint64_t>(V) + 1));
+    const unsigned tiles = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(L, 1024), cap)));
+    const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(L, 256), cap)));
+    const unsigned vgrid =
+        static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(static_cast<uint64_t>(V) + 1, 256), cap));
+    if (L > 0)
+        GCU_LAUNCH(dev, "kt_live_flag", kt_live_flag_kernel, tiles, 256, 0, lv, V, L, rev, state, pos.ptr);
+    GCU_TRY(exclusive_scan_u32(dev, pos.ptr, pos.ptr, L));
+    GCU_LAUNCH(dev, "kt_live_offsets", kt_live_offsets_kernel, vgrid, 256, 0, lv.offsets, V, pos.ptr,
+               out->offsets.ptr);
+    GCU_CUDA(cudaMemcpyAsync(&out->entries, pos.ptr + L, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream),
+             "copy");
+    GCU_TRY(dev.sync());
+    GCU_TRY(out->targets.allocate(dev, std::max<uint32_t>(out->entries, 1)));
+    GCU_TRY(out->eid.allocate(dev, std::max<uint32_t>(out->entries, 1)));
+    if (out->entries > 0)
+        GCU_LAUNCH(dev, "kt_live_fill", kt_live_fill_kernel, grid, 256, 0, lv, L, pos.ptr, out->targets.ptr,
+                   out->eid.ptr);
+    GCU_TRY(dev.sync());  // pos is freed on return
+    return ok();
+}
+
+// The entries listed for round r are removed in it (state = r); with truss,
+// they also get truss_value.
+__global__ void kt_mark_kernel(const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
+                               uint32_t* __restrict__ state, uint32_t round, uint32_t* __restrict__ truss,
+                               uint32_t truss_value) {
+    const uint32_t n = *count;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t j = list[i];
+        state[j] = round;
+        if (truss) truss[j] = truss_value;
     }
 }
 
@@ -381,11 +547,15 @@ static Error k_truss_symmetric(GraphImpl& g, uint32_t k, std::vector<uint32_t>* 
     GCU_TRY(ensure_kt_cache(g, &c));
     const uint32_t* src = c->src.ptr;
     const uint32_t* rev = c->rev.ptr;
-    DeviceBuffer<uint32_t> support, state, removed, scratch;
+    DeviceBuffer<uint32_t> support, state, removed, scratch, lists[2];
     GCU_TRY(support.allocate(dev, static_cast<uint64_t>(E) + 1));
     GCU_TRY(state.allocate(dev, static_cast<uint64_t>(E) + 1));
     GCU_TRY(removed.allocate(dev, E));
-    GCU_TRY(scratch.allocate(dev, 1));  // removed this round
+    GCU_TRY(lists[0].allocate(dev, E));
+    GCU_TRY(lists[1].allocate(dev, E));
+    DeviceBuffer<uint32_t> chunks;  // peel chunk counts, then their scan
+    GCU_TRY(chunks.allocate(dev, static_cast<uint64_t>(E) + 1));
+    GCU_TRY(scratch.allocate(dev, 3));  // [0] removed by a scan, [1 + b] entries of lists[b]
     GCU_CUDA(cudaMemcpyAsync(support.ptr, c->support.ptr, sizeof(uint32_t) * static_cast<size_t>(E),
                              cudaMemcpyDeviceToDevice, dev.stream),
              "copy");
@@ -394,23 +564,51 @@ static Error k_truss_symmetric(GraphImpl& g, uint32_t k, std::vector<uint32_t>* 
     const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
     const uint32_t loops = c->loops;
 
+    // Rounds 1 and (with self-loops) 2 scan every entry: round 1 adds the
+    // self-loop terms, so an edge it keeps may be below the threshold in
+    // round 2 without losing a triangle. Later rounds remove exactly the
+    // edges that the previous round's peel brought below the threshold.
     uint32_t round = 1;
+    int cur = 0;       // the peel of this round lists the next round's removals in lists[cur]
+    uint32_t n = 0;    // entries removed in this round
     while (true) {
-        GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
-        GCU_LAUNCH(dev, "kt_round_filter", kt_round_filter_kernel, edge_grid, 256, 0, g.targets.ptr, src,
-                   c->loop.ptr, support.ptr, state.ptr, E, threshold, round, removed.ptr, scratch.ptr, nullptr, 0u);
-        uint32_t n = 0;
-        GCU_CUDA(cudaMemcpyAsync(&n, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
-        GCU_TRY(dev.sync());
+        const bool scan = round == 1 || (round == 2 && loops > 0);
+        const uint32_t* list = removed.ptr;
+        const uint32_t* count = scratch.ptr;
+        if (scan) {
+            GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
+            GCU_LAUNCH(dev, "kt_round_filter", kt_round_filter_kernel, edge_grid, 256, 0, g.targets.ptr, src,
+                       c->loop.ptr, support.ptr, state.ptr, E, threshold, round, removed.ptr, scratch.ptr, nullptr,
+                       0u);
+            GCU_CUDA(cudaMemcpyAsync(&n, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+            GCU_TRY(dev.sync());
+        } else {
+            // n = the previous peel's list (read below); mark it removed in this round.
+            list = lists[cur ^ 1].ptr;
+            count = scratch.ptr + 1 + (cur ^ 1);
+            if (n > 0) {
+                const unsigned grid =
+                    static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(n, 256), cap));
+                GCU_LAUNCH(dev, "kt_mark", kt_mark_kernel, grid, 256, 0, list, count, state.ptr, round,
+                           static_cast<uint32_t*>(nullptr), 0u);
+            }
+        }
         // Round 1 also removes the self-loop entries (their support is 0).
         const bool removed_any = n > 0 || (round == 1 && loops > 0);
         if (!removed_any) break;
+        uint32_t next_n = 0;
+        GCU_CUDA(cudaMemsetAsync(scratch.ptr + 1 + cur, 0, sizeof(uint32_t), dev.stream), "memset");
         if (n > 0) {
-            const unsigned peel_grid =
-                static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(static_cast<uint64_t>(n) * 32, 256), cap));
-            GCU_LAUNCH(dev, "kt_peel", kt_peel_kernel, peel_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src, rev,
-                       state.ptr, support.ptr, removed.ptr, scratch.ptr, round);
+            GCU_TRY(launch_peel(dev, g, LiveCsr{g.offsets.ptr, g.targets.ptr, nullptr}, src, rev, state.ptr,
+                                support.ptr, list, count, n, chunks.ptr, round, threshold, lists[cur].ptr,
+                                scratch.ptr + 1 + cur));
+            GCU_CUDA(cudaMemcpyAsync(&next_n, scratch.ptr + 1 + cur, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                     dev.stream),
+                     "copy");
+            GCU_TRY(dev.sync());
         }
+        n = next_n;
+        cur ^= 1;
         round += 1;
     }
     *iterations = round;
@@ -528,12 +726,16 @@ Error truss_decomposition(GraphImpl& g, uint32_t* host_truss, uint32_t* max_trus
     GCU_TRY(ensure_kt_cache(g, &c));
     const uint32_t* src = c->src.ptr;
     const uint32_t* rev = c->rev.ptr;
-    DeviceBuffer<uint32_t> support, state, removed, truss, scratch, active[2];
+    DeviceBuffer<uint32_t> support, state, removed, truss, scratch, active[2], lists[2];
     GCU_TRY(support.allocate(dev, E));
     GCU_TRY(state.allocate(dev, E));
     GCU_TRY(removed.allocate(dev, E));
     GCU_TRY(truss.allocate(dev, E));
-    GCU_TRY(scratch.allocate(dev, 2));  // [0] removed this round, [1] active count
+    GCU_TRY(lists[0].allocate(dev, E));
+    GCU_TRY(lists[1].allocate(dev, E));
+    DeviceBuffer<uint32_t> chunks;  // peel chunk counts, then their scan
+    GCU_TRY(chunks.allocate(dev, static_cast<uint64_t>(E) + 1));
+    GCU_TRY(scratch.allocate(dev, 4));  // [0] removed by a scan, [1] active count, [2 + b] entries of lists[b]
     const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
     const unsigned edge_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(E, 256), cap));
     GCU_CUDA(cudaMemcpyAsync(support.ptr, c->support.ptr, sizeof(uint32_t) * static_cast<size_t>(E),
@@ -552,37 +754,70 @@ Error truss_decomposition(GraphImpl& g, uint32_t* host_truss, uint32_t* max_trus
     GCU_CUDA(cudaMemsetAsync(scratch.ptr + 1, 0, sizeof(uint32_t), dev.stream), "memset");
     GCU_LAUNCH(dev, "kt_active", kt_active_kernel, edge_grid, 256, 0, g.targets.ptr, src, state.ptr,
                static_cast<const uint32_t*>(nullptr), E, active[0].ptr, scratch.ptr + 1);
-    int cur = 0;
+    int cur = 0;              // active list in use
+    int out = 0;              // the peel lists the next round's removals in lists[out]
+    LiveCsr live{g.offsets.ptr, g.targets.ptr, nullptr};  // the peel's lists
+    uint32_t live_entries = E;
+    LiveBuffers live_bufs[2];
+    int live_cur = 0;
     uint64_t listed = alive;  // entries in active[cur]
     uint32_t round = 0, k = 3, top = alive > 0 ? 2 : 0;
+    // The first round of every level scans the active list for the edges
+    // below the new threshold; every later round of the level removes
+    // exactly the edges that the previous peel brought below it.
+    bool level_start = true;
+    uint32_t n = 0;  // entries removed in this round
     while (alive > 0) {
         round += 1;
         const unsigned grid =
             static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(listed, 256), cap)));
-        GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
-        GCU_LAUNCH(dev, "kt_active_filter", kt_active_filter_kernel, grid, 256, 0, active[cur].ptr,
-                   static_cast<uint32_t>(listed), support.ptr, state.ptr, k - 2, round, removed.ptr, scratch.ptr,
-                   truss.ptr, k - 1);
-        uint32_t n = 0;
-        GCU_CUDA(cudaMemcpyAsync(&n, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
-        GCU_TRY(dev.sync());
+        const uint32_t* list = removed.ptr;
+        const uint32_t* count = scratch.ptr;
+        if (level_start) {
+            GCU_CUDA(cudaMemsetAsync(scratch.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
+            GCU_LAUNCH(dev, "kt_active_filter", kt_active_filter_kernel, grid, 256, 0, active[cur].ptr,
+                       static_cast<uint32_t>(listed), support.ptr, state.ptr, k - 2, round, removed.ptr,
+                       scratch.ptr, truss.ptr, k - 1);
+            GCU_CUDA(cudaMemcpyAsync(&n, scratch.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream), "copy");
+            GCU_TRY(dev.sync());
+        } else {
+            list = lists[out ^ 1].ptr;
+            count = scratch.ptr + 2 + (out ^ 1);
+            if (n > 0) {
+                const unsigned mark_grid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(n, 256), cap));
+                GCU_LAUNCH(dev, "kt_mark", kt_mark_kernel, mark_grid, 256, 0, list, count, state.ptr, round,
+                           truss.ptr, k - 1);
+            }
+        }
         if (n == 0) {
             // Every alive edge has at least k - 2 alive triangles: it is in the k-truss.
             top = k;
             k += 1;
+            level_start = true;
             continue;
         }
         alive -= n;
-        const unsigned peel_grid =
-            static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(static_cast<uint64_t>(n) * 32, 256), cap));
-        GCU_LAUNCH(dev, "kt_peel", kt_peel_kernel, peel_grid, 256, 0, g.offsets.ptr, g.targets.ptr, src, rev,
-                   state.ptr, support.ptr, removed.ptr, scratch.ptr, round);
+        GCU_CUDA(cudaMemsetAsync(scratch.ptr + 2 + out, 0, sizeof(uint32_t), dev.stream), "memset");
+        GCU_TRY(launch_peel(dev, g, live, src, rev, state.ptr, support.ptr, list, count, n, chunks.ptr, round, k - 2,
+                            lists[out].ptr, scratch.ptr + 2 + out));
+        GCU_CUDA(cudaMemcpyAsync(&n, scratch.ptr + 2 + out, sizeof(uint32_t), cudaMemcpyDeviceToHost, dev.stream),
+                 "copy");
+        GCU_TRY(dev.sync());
+        out ^= 1;
+        level_start = false;
         if (alive > 0 && 2 * alive < listed) {
             GCU_CUDA(cudaMemsetAsync(scratch.ptr + 1, 0, sizeof(uint32_t), dev.stream), "memset");
             GCU_LAUNCH(dev, "kt_active", kt_active_kernel, grid, 256, 0, g.targets.ptr, src, state.ptr,
                        active[cur].ptr, static_cast<uint32_t>(listed), active[cur ^ 1].ptr, scratch.ptr + 1);
             cur ^= 1;
             listed = alive;
+            // The peel's lists too: the alive entries only (the removals
+            // listed for the next round are still alive and stay).
+            GCU_TRY(compact_live(dev, g.num_nodes, live, live_entries, rev, state.ptr, &live_bufs[live_cur ^ 1]));
+            live_cur ^= 1;
+            live = LiveCsr{live_bufs[live_cur].offsets.ptr, live_bufs[live_cur].targets.ptr,
+                           live_bufs[live_cur].eid.ptr};
+            live_entries = live_bufs[live_cur].entries;
         }
     }
     *max_truss = top;
