@@ -42,11 +42,12 @@ HELDOUT_SEED_BASE = 1_000_000  # held-out graph seeds start here; training seeds
 
 
 def corpus(count: int, seed: int, scale_range=(16, 22)) -> list[dict]:
-    """Seeded graph specs, one third each R-MAT, grid, geometric."""
+    """Seeded graph specs, one quarter each R-MAT, grid, geometric and
+    Erdos-Renyi (uniform neighbours: no hubs and no locality)."""
     rng = np.random.default_rng(seed)
     specs = []
     for i in range(count):
-        kind = ("rmat", "grid", "geometric")[i % 3]
+        kind = ("rmat", "grid", "geometric", "erdos_renyi")[i % 4]
         gseed = int(seed * 100_003 + i)
         if kind == "rmat":
             a = float(rng.uniform(0.45, 0.65))
@@ -56,9 +57,12 @@ def corpus(count: int, seed: int, scale_range=(16, 22)) -> list[dict]:
             lo, hi = 2 ** (scale_range[0] // 2), 2 ** ((scale_range[1] + 1) // 2)
             specs.append({"kind": kind, "width": int(rng.integers(lo, hi + 1)), "height": int(rng.integers(lo, hi + 1)),
                           "drop": 0.05, "seed": gseed})
-        else:
+        elif kind == "geometric":
             specs.append({"kind": kind, "n": int(2 ** rng.integers(scale_range[0], scale_range[1])),
                           "avg_degree": float(rng.uniform(8, 64)), "seed": gseed})
+        else:
+            n = int(2 ** rng.integers(scale_range[0], scale_range[1] + 1))
+            specs.append({"kind": kind, "n": n, "pairs": int(n * rng.uniform(4, 32)), "seed": gseed})
     return specs
 
 
@@ -70,6 +74,8 @@ def make_graph(device: G.GpuDevice, spec: dict) -> G.GpuGraph:
         return G.GpuGraph.generate_grid(device, spec["width"], spec["height"], spec["drop"], spec["seed"])
     if k == "geometric":
         return G.GpuGraph.generate_geometric(device, spec["n"], spec["avg_degree"], spec["seed"])
+    if k == "erdos_renyi":
+        return G.GpuGraph.generate_erdos_renyi(device, spec["n"], spec["pairs"], spec["seed"])
     raise ValueError(f"unknown graph kind {k!r}")
 
 
