@@ -18,8 +18,10 @@
 //    original one.
 //  * Rows of one class have similar length, so each class gets a fixed group
 //    of 2^(c-1) lanes per row (1 to 32); a group works on 2 rows in lockstep,
-//    4 steps per trip, so every lane keeps 8 independent loads in flight within
-//    32 registers (8 CTAs per SM, persistent); consecutive groups read
+//    2 steps per trip (a row of class c has fewer than 2g entries, so a third
+//    step would always be masked below class 6), so every lane keeps 4
+//    independent loads in flight within 32 registers (8 CTAs per SM,
+//    persistent); consecutive groups read
 //    consecutive rows (coalesced), and there is no search, staging, barrier or
 //    carry. Rows of 1024 or more entries are split into 1024-entry segments,
 //    one warp each, and their partial sums are added in segment order by the
@@ -57,7 +59,7 @@ constexpr uint32_t kSegment = 1024;   // entries per long-row segment (one warp)
 constexpr int kClassBlock = 1024;     // vertices per block of the class partition
 constexpr int kMaxPhases = 16;
 constexpr int kRowsPerGroup = 2;      // rows a lane group works on in lockstep
-constexpr int kUnroll = 4;            // steps per loop trip: kRowsPerGroup * kUnroll loads in flight
+constexpr int kUnroll = 2;            // steps per loop trip: kRowsPerGroup * kUnroll loads in flight
 constexpr int kRowCtasPerSm = 8;      // persistent CTAs of the row kernel per SM
 
 enum : uint32_t { kPhaseLong = 0, kPhaseGroup = 1, kPhaseEmpty = 2 };
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
     unsigned long long* __restrict__ row_partials) {
     if (state->done) return;
     // Loop invariants live in shared memory, so that the unrolled gather loop
-    // keeps its 8 loads in flight within 32 registers; the fixed-point sums
+    // keeps its loads in flight within 32 registers; the fixed-point sums
     // stay in registers per lane until the end.
     constexpr int kWarps = kPrThreads / 32;
     __shared__ double s_mass[2];                     // dangling mass, its uniform share
@@ -377,8 +379,8 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
             } else if (ph.kind == kPhaseGroup) {
                 // Rows of one class, 2^log2g lanes per row, kRowsPerGroup rows per
                 // group worked on in lockstep: each step issues one target load and
-                // one gather per row (8 in flight per lane with the kUnroll-step
-                // unroll), so no row waits on the previous one's memory round trips.
+                // one gather per row (kRowsPerGroup * kUnroll in flight per lane),
+                // so no row waits on the previous one's memory round trips.
                 const uint32_t log2g = ph.log2g, g = 1u << log2g;
                 const uint32_t groups = 32u >> log2g;
                 const uint32_t group = lane >> log2g, lig = lane & (g - 1);
