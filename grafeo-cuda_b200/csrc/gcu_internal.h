@@ -90,6 +90,8 @@ struct DeviceImpl {
     cudaStream_t stream = nullptr;
     cudaEvent_t timer_start = nullptr;
     cudaEvent_t timer_stop = nullptr;
+    cudaStream_t copy_stream = nullptr;  // chunked host-to-device copies that overlap the checks
+    cudaEvent_t copy_event = nullptr;
 
     std::atomic<uint64_t> launches{0};
     bool kernel_timing = false;
@@ -207,6 +209,12 @@ std::string describe_node_violation(uint32_t node, uint32_t start, uint32_t end,
 // Finds the first node that breaks a CSR rule on the device; UINT32_MAX if none.
 Error validate_csr_device(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets,
                           uint32_t num_nodes, uint32_t num_edges, uint32_t* first_bad_node);
+// The same checks while copying the targets from the host: the offsets are
+// already on the device (or queued on dev.stream); the targets go up in chunks
+// on dev.copy_stream and each chunk's entries are checked as soon as it lands.
+Error upload_and_validate_csr(DeviceImpl& dev, const uint32_t* d_offsets, uint32_t* d_targets,
+                              const uint32_t* h_targets, uint32_t num_nodes, uint32_t num_edges,
+                              uint32_t* first_bad_node);
 
 // Whether every entry u -> v has its reverse v -> u (cached on the graph).
 Error graph_symmetry(GraphImpl& g, bool* symmetric);

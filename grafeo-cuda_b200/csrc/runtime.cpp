@@ -64,6 +64,11 @@ DeviceImpl::~DeviceImpl() {
     for (auto e : event_pool) cudaEventDestroy(e);
     if (timer_start) cudaEventDestroy(timer_start);
     if (timer_stop) cudaEventDestroy(timer_stop);
+    if (copy_stream) {
+        cudaStreamSynchronize(copy_stream);
+        cudaStreamDestroy(copy_stream);
+    }
+    if (copy_event) cudaEventDestroy(copy_event);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -191,6 +196,8 @@ static Error create_device(int ordinal, std::shared_ptr<DeviceImpl>* out) {
     GCU_CUDA(cudaStreamCreateWithFlags(&dev->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     GCU_CUDA(cudaEventCreate(&dev->timer_start), "cudaEventCreate");
     GCU_CUDA(cudaEventCreate(&dev->timer_stop), "cudaEventCreate");
+    GCU_CUDA(cudaStreamCreateWithFlags(&dev->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    GCU_CUDA(cudaEventCreateWithFlags(&dev->copy_event, cudaEventDisableTiming), "cudaEventCreate");
     // Keep freed stream-ordered allocations cached in the pool, so repeated
     // algorithm calls do not return memory to the driver between calls.
     cudaMemPool_t pool;
@@ -378,12 +385,11 @@ GCU_API gcu_status gcu_graph_from_csr(gcu_device* dev, const uint32_t* offsets, 
     if (e.ok()) e = g->targets.allocate(d, n_targets);
     if (!e.ok()) return fail(e);
     cudaError_t c = cudaMemcpyAsync(g->offsets.ptr, offsets, n_offsets * 4, cudaMemcpyHostToDevice, d.stream);
-    if (c == cudaSuccess && n_targets)
-        c = cudaMemcpyAsync(g->targets.ptr, targets, n_targets * 4, cudaMemcpyHostToDevice, d.stream);
     if (c != cudaSuccess) return fail(driver_error(c, "copy CSR to device"));
 
+    // The targets are copied in chunks that the entry checks follow.
     uint32_t bad = UINT32_MAX;
-    e = validate_csr_device(d, g->offsets.ptr, g->targets.ptr, g->num_nodes, g->num_edges, &bad);
+    e = upload_and_validate_csr(d, g->offsets.ptr, g->targets.ptr, targets, g->num_nodes, g->num_edges, &bad);
     if (!e.ok()) return fail(e);
     if (bad != UINT32_MAX) {
         // Reproduce the exact reference message for that node on the host.

@@ -50,12 +50,14 @@ __global__ void csr_mark_starts_kernel(const uint32_t* __restrict__ offsets, uin
     }
 }
 
+// Entries [j0, j1) (those below the first offset violation); entry j - 1 must
+// be on the device too.
 __global__ void csr_check_entries_kernel(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
                                          uint32_t V, const uint32_t* __restrict__ starts,
-                                         uint32_t* __restrict__ flags) {
+                                         uint32_t* __restrict__ flags, uint64_t j0, uint64_t j1) {
     const uint32_t limit = checked_limit(flags, V);
-    const uint32_t end = offsets[limit];
-    for (uint64_t j = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < end;
+    const uint64_t end = min_u64(offsets[limit], j1);
+    for (uint64_t j = j0 + static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < end;
          j += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint32_t t = ld_stream(targets + j);
         const bool first = (starts[j >> 5] >> (j & 31)) & 1u;
@@ -64,10 +66,21 @@ __global__ void csr_check_entries_kernel(const uint32_t* __restrict__ offsets, c
     }
 }
 
-Error validate_csr_device(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets,
-                          uint32_t num_nodes, uint32_t num_edges, uint32_t* first_bad_node) {
+// Entries per chunk of the overlapped upload (64 MB of targets).
+constexpr uint64_t kUploadChunk = uint64_t{1} << 24;
+
+// With h_targets, the targets are copied here, chunk by chunk on the copy
+// stream, and the entry checks of each chunk wait for its copy only.
+static Error check_csr(DeviceImpl& dev, const uint32_t* d_offsets, uint32_t* d_targets, const uint32_t* h_targets,
+                       uint32_t num_nodes, uint32_t num_edges, uint32_t* first_bad_node) {
     *first_bad_node = UINT32_MAX;
-    if (num_nodes == 0) return ok();
+    if (num_nodes == 0) {
+        if (h_targets && num_edges)
+            GCU_CUDA(cudaMemcpyAsync(d_targets, h_targets, sizeof(uint32_t) * num_edges, cudaMemcpyHostToDevice,
+                                     dev.stream),
+                     "copy CSR to device");
+        return ok();
+    }
     const uint64_t words = ceil_div_u64(num_edges, 32);
     DeviceBuffer<uint32_t> scratch;  // 4 flags, then the list-start bitmap
     GCU_TRY(scratch.allocate(dev, 4 + words));
@@ -82,13 +95,55 @@ Error validate_csr_device(DeviceImpl& dev, const uint32_t* d_offsets, const uint
                flags);
     GCU_LAUNCH(dev, "csr_mark_starts", csr_mark_starts_kernel, node_grid, 256, 0, d_offsets, num_nodes, flags,
                starts);
-    GCU_LAUNCH(dev, "csr_check_entries", csr_check_entries_kernel, entry_grid, 256, 0, d_offsets, d_targets,
-               num_nodes, starts, flags);
+    if (!h_targets) {
+        GCU_LAUNCH(dev, "csr_check_entries", csr_check_entries_kernel, entry_grid, 256, 0, d_offsets, d_targets,
+                   num_nodes, starts, flags, uint64_t{0}, static_cast<uint64_t>(num_edges));
+    } else if (num_edges > 0) {
+        // The copy stream starts once the buffers above exist (they are
+        // stream-ordered allocations of dev.stream); dev.stream then waits for
+        // each chunk before checking it.
+        GCU_CUDA(cudaEventRecord(dev.copy_event, dev.stream), "cudaEventRecord");
+        GCU_CUDA(cudaStreamWaitEvent(dev.copy_stream, dev.copy_event, 0), "cudaStreamWaitEvent");
+        Error err = ok();
+        for (uint64_t c0 = 0; c0 < num_edges && err.ok(); c0 += kUploadChunk) {
+            const uint64_t c1 = std::min<uint64_t>(c0 + kUploadChunk, num_edges);
+            cudaError_t c = cudaMemcpyAsync(d_targets + c0, h_targets + c0, sizeof(uint32_t) * (c1 - c0),
+                                            cudaMemcpyHostToDevice, dev.copy_stream);
+            if (c == cudaSuccess) c = cudaEventRecord(dev.copy_event, dev.copy_stream);
+            if (c == cudaSuccess) c = cudaStreamWaitEvent(dev.stream, dev.copy_event, 0);
+            if (c != cudaSuccess) {
+                err = driver_error(c, "copy CSR to device");
+                break;
+            }
+            const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(c1 - c0, 256), cap)));
+            err = [&]() -> Error {
+                GCU_LAUNCH(dev, "csr_check_entries", csr_check_entries_kernel, grid, 256, 0, d_offsets, d_targets,
+                           num_nodes, starts, flags, c0, c1);
+                return ok();
+            }();
+        }
+        if (!err.ok()) {
+            cudaStreamSynchronize(dev.copy_stream);  // no copy may outlive the buffers
+            return err;
+        }
+    }
     uint32_t host[4];
     GCU_CUDA(cudaMemcpyAsync(host, flags, sizeof(host), cudaMemcpyDeviceToHost, dev.stream), "copy flags");
     GCU_TRY(dev.sync());
     *first_bad_node = std::min(std::min(host[0], host[1]), host[2]);
     return ok();
+}
+
+Error validate_csr_device(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets,
+                          uint32_t num_nodes, uint32_t num_edges, uint32_t* first_bad_node) {
+    return check_csr(dev, d_offsets, const_cast<uint32_t*>(d_targets), nullptr, num_nodes, num_edges,
+                     first_bad_node);
+}
+
+Error upload_and_validate_csr(DeviceImpl& dev, const uint32_t* d_offsets, uint32_t* d_targets,
+                              const uint32_t* h_targets, uint32_t num_nodes, uint32_t num_edges,
+                              uint32_t* first_bad_node) {
+    return check_csr(dev, d_offsets, d_targets, h_targets, num_nodes, num_edges, first_bad_node);
 }
 
 // Symmetry test: every entry u -> v needs v -> u; each entry binary-searches

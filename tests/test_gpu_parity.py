@@ -129,6 +129,33 @@ def test_invalid_csr_messages_match_host_validation(device):
         assert host == dev, (offsets.tolist(), targets.tolist())
 
 
+def test_chunked_upload_checks_every_chunk(device):
+    """from_csr copies the targets in 16M-entry chunks and checks each chunk
+    as it lands: a violation in the third chunk, at a chunk boundary, or in
+    the first entry of a chunk is reported like the host validator does, and
+    a valid graph of several chunks comes back entry for entry."""
+    n, deg = 1 << 20, 40  # 41,943,040 entries: three chunks
+    offsets = np.arange(n + 1, dtype=np.uint32) * deg
+    base = (np.arange(n, dtype=np.uint64)[:, None] * 7 + np.arange(deg, dtype=np.uint64)[None, :] * 26_000)
+    targets = (base % n).astype(np.uint32)
+    targets.sort(axis=1)
+    targets = np.ascontiguousarray(targets.reshape(-1))
+    g = G.GpuGraph.from_csr(offsets, targets, device)
+    back = g.to_csr()
+    assert np.array_equal(back.offsets, offsets) and np.array_equal(back.targets, targets)
+    del g
+    chunk = 1 << 24
+    for j in (36_000_000, chunk, 2 * chunk - 1, 2 * chunk):
+        bad = targets.copy()
+        row = j // deg
+        bad[j] = bad[j - 1] if j % deg else n  # a repeat inside the list, or past the end at a list start
+        with pytest.raises(GrafeoCudaError) as host:
+            G.validate_csr(offsets, bad)
+        with pytest.raises(GrafeoCudaError) as dev:
+            G.GpuGraph.from_csr(offsets, bad, device)
+        assert str(dev.value) == str(host.value), (j, row)
+
+
 def test_argument_errors(device):
     g = upload(device, *graphs.K4_CSR)
     with pytest.raises(GrafeoCudaError) as e:
