@@ -216,6 +216,11 @@ Error upload_and_validate_csr(DeviceImpl& dev, const uint32_t* d_offsets, uint32
                               const uint32_t* h_targets, uint32_t num_nodes, uint32_t num_edges,
                               uint32_t* first_bad_node);
 
+// New id of every vertex in the stable partition by degree class (class c:
+// list lengths in [2^(c-1), 2^c)), highest class first: the order the
+// PageRank plan relabels by, and the triangle count orients by.
+Error degree_class_order(DeviceImpl& dev, const uint32_t* offsets, uint32_t V, DeviceBuffer<uint32_t>* inv);
+
 // Whether every entry u -> v has its reverse v -> u (cached on the graph).
 Error graph_symmetry(GraphImpl& g, bool* symmetric);
 

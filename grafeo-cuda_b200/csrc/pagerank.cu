@@ -193,6 +193,22 @@ __global__ void pr_perm_degree_kernel(const uint32_t* __restrict__ offsets, cons
     }
 }
 
+Error degree_class_order(DeviceImpl& dev, const uint32_t* offsets, uint32_t V, DeviceBuffer<uint32_t>* inv) {
+    GCU_TRY(inv->allocate(dev, std::max<uint32_t>(V, 1)));
+    if (V == 0) return ok();
+    const uint32_t nblk = static_cast<uint32_t>(ceil_div_u64(V, kClassBlock));
+    const uint64_t ncount = static_cast<uint64_t>(kDegClasses) * nblk;
+    DeviceBuffer<uint32_t> counts, cpos, perm;
+    GCU_TRY(counts.allocate(dev, ncount));
+    GCU_TRY(cpos.allocate(dev, ncount + 1));
+    GCU_TRY(perm.allocate(dev, V));
+    GCU_LAUNCH(dev, "pr_class_count", pr_class_count_kernel, nblk, kClassBlock, 0, offsets, V, nblk, counts.ptr);
+    GCU_TRY(exclusive_scan_u32(dev, counts.ptr, cpos.ptr, ncount));
+    GCU_LAUNCH(dev, "pr_class_scatter", pr_class_scatter_kernel, nblk, kClassBlock, 0, offsets, V, nblk, cpos.ptr,
+               perm.ptr, inv->ptr);
+    return ok();
+}
+
 // Relabelled CSR entry k of row r is original entry offsets[perm[r]] +
 // (k - poff[r]) with its target renamed. Blocks work on tiles of consecutive
 // output entries (rows found through the staged row starts), so a hub's list

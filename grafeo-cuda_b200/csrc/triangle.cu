@@ -60,9 +60,12 @@ constexpr int kOrientThreads = 256;
 constexpr int kOrientItems = 4;
 constexpr int kOrientTile = kOrientThreads * kOrientItems;  // entries per tile
 
+// With `rank`, u -> v is kept when v ranks below u (the orientation is that
+// vertex order) and by_degree is ignored.
 __global__ void __launch_bounds__(kOrientThreads) tc_orient_flag_kernel(const uint32_t* __restrict__ offsets,
                                                                         const uint32_t* __restrict__ targets,
                                                                         uint32_t V, uint32_t E, bool by_degree,
+                                                                        const uint32_t* __restrict__ rank,
                                                                         uint32_t* __restrict__ keep) {
     __shared__ uint32_t s_start[kOrientTile];
     __shared__ uint32_t s_meta[2];
@@ -76,24 +79,31 @@ __global__ void __launch_bounds__(kOrientThreads) tc_orient_flag_kernel(const ui
             const uint64_t j = e0 + q * kOrientThreads + threadIdx.x;
             if (j >= e1) continue;
             const uint32_t u = tile_row(offsets, V, s_start, staged, r0, nrows, static_cast<uint32_t>(j));
-            const uint32_t du = __ldg(offsets + u + 1) - __ldg(offsets + u);
             const uint32_t v = ld_stream(targets + j);
-            const uint32_t dv = __ldg(offsets + v + 1) - __ldg(offsets + v);
-            keep[j] = dag_keep(u, du, v, dv, by_degree) ? 1u : 0u;
+            if (rank) {
+                keep[j] = __ldg(rank + v) < __ldg(rank + u) ? 1u : 0u;
+            } else {
+                const uint32_t du = __ldg(offsets + u + 1) - __ldg(offsets + u);
+                const uint32_t dv = __ldg(offsets + v + 1) - __ldg(offsets + v);
+                keep[j] = dag_keep(u, du, v, dv, by_degree) ? 1u : 0u;
+            }
         }
         __syncthreads();  // the staged starts are rewritten for the next tile
     }
 }
 
 // Kept entries to their DAG positions; with dag_eid, also the CSR index of
-// the edge's u < v entry (the undirected edge id).
+// the edge's u < v entry (the undirected edge id); with dag_rank, the rank of
+// each kept target.
 __global__ void __launch_bounds__(kOrientThreads) tc_orient_fill_kernel(const uint32_t* __restrict__ offsets,
                                                                         const uint32_t* __restrict__ targets,
                                                                         uint32_t V, uint32_t E,
                                                                         const uint32_t* __restrict__ pos,
                                                                         uint32_t* __restrict__ dag_targets,
                                                                         const uint32_t* __restrict__ rev,
-                                                                        uint32_t* __restrict__ dag_eid) {
+                                                                        uint32_t* __restrict__ dag_eid,
+                                                                        const uint32_t* __restrict__ rank,
+                                                                        uint32_t* __restrict__ dag_rank) {
     __shared__ uint32_t s_start[kOrientTile];
     __shared__ uint32_t s_meta[2];
     for (uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kOrientTile; e0 < E;
@@ -109,6 +119,7 @@ __global__ void __launch_bounds__(kOrientThreads) tc_orient_fill_kernel(const ui
             if (pos[j + 1] == at) continue;
             const uint32_t v = ld_stream(targets + j);
             dag_targets[at] = v;
+            if (dag_rank) dag_rank[at] = __ldg(rank + v);
             if (dag_eid) {
                 const uint32_t u = tile_row(offsets, V, s_start, staged, r0, nrows, static_cast<uint32_t>(j));
                 dag_eid[at] = u < v ? static_cast<uint32_t>(j) : rev[j];
@@ -145,8 +156,11 @@ struct CountSink {
 
 }  // namespace
 
-Error build_dag(GraphImpl& g, bool by_degree, const uint32_t* rev, DeviceBuffer<uint32_t>* dag_offsets,
-                DeviceBuffer<uint32_t>* dag_targets, DeviceBuffer<uint32_t>* dag_eid, uint32_t* m) {
+// With `rank`: oriented by that vertex order, and dag_rank (when given) holds
+// the rank of every DAG target.
+static Error build_dag_impl(GraphImpl& g, bool by_degree, const uint32_t* rank, const uint32_t* rev,
+                            DeviceBuffer<uint32_t>* dag_offsets, DeviceBuffer<uint32_t>* dag_targets,
+                            DeviceBuffer<uint32_t>* dag_eid, DeviceBuffer<uint32_t>* dag_rank, uint32_t* m) {
     DeviceImpl& dev = *g.dev;
     const uint32_t V = g.num_nodes, E = g.num_edges;
     GCU_TRY(dag_offsets->allocate(dev, static_cast<uint64_t>(V) + 1));
@@ -158,7 +172,7 @@ Error build_dag(GraphImpl& g, bool by_degree, const uint32_t* rev, DeviceBuffer<
     const unsigned vgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(static_cast<uint64_t>(V) + 1, 256), cap));
     if (E > 0)
         GCU_LAUNCH(dev, "tc_orient_flag", tc_orient_flag_kernel, tiles, kOrientThreads, 0, g.offsets.ptr,
-                   g.targets.ptr, V, E, by_degree, pos.ptr);
+                   g.targets.ptr, V, E, by_degree, rank, pos.ptr);
     GCU_TRY(exclusive_scan_u32(dev, pos.ptr, pos.ptr, E));
     GCU_LAUNCH(dev, "tc_orient_offsets", tc_orient_offsets_kernel, vgrid, 256, 0, g.offsets.ptr, V, pos.ptr,
                dag_offsets->ptr);
@@ -166,11 +180,18 @@ Error build_dag(GraphImpl& g, bool by_degree, const uint32_t* rev, DeviceBuffer<
     GCU_TRY(dev.sync());
     GCU_TRY(dag_targets->allocate(dev, std::max<uint32_t>(*m, 1)));
     if (dag_eid) GCU_TRY(dag_eid->allocate(dev, std::max<uint32_t>(*m, 1)));
+    if (dag_rank) GCU_TRY(dag_rank->allocate(dev, std::max<uint32_t>(*m, 1)));
     if (*m == 0) return ok();
     GCU_LAUNCH(dev, "tc_orient_fill", tc_orient_fill_kernel, tiles, kOrientThreads, 0, g.offsets.ptr, g.targets.ptr,
-               V, E, pos.ptr, dag_targets->ptr, rev, dag_eid ? dag_eid->ptr : nullptr);
+               V, E, pos.ptr, dag_targets->ptr, rev, dag_eid ? dag_eid->ptr : nullptr, rank,
+               dag_rank ? dag_rank->ptr : nullptr);
     GCU_TRY(dev.sync());  // pos is freed on return
     return ok();
+}
+
+Error build_dag(GraphImpl& g, bool by_degree, const uint32_t* rev, DeviceBuffer<uint32_t>* dag_offsets,
+                DeviceBuffer<uint32_t>* dag_targets, DeviceBuffer<uint32_t>* dag_eid, uint32_t* m) {
+    return build_dag_impl(g, by_degree, nullptr, rev, dag_offsets, dag_targets, dag_eid, nullptr, m);
 }
 
 // ---------------------------------------------------------------- out-degree buckets
@@ -305,9 +326,12 @@ Error plan_buckets(DeviceImpl& dev, const uint32_t* d_offsets, uint32_t V, uint3
 }
 
 // One launch of `variant` over bucket c's vertices; next = its handout counter (zeroed).
+// rank / vrank (a DAG oriented by a vertex order: the rank of every entry's
+// target, of every vertex) let the CTA variants use rank bitmaps; nullptr
+// for any other DAG.
 template <class Sink>
 Error launch_bucket(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets, const BucketPlan& p, int c,
-                    int variant, uint32_t* next, bool split, Sink sink) {
+                    int variant, uint32_t* next, bool split, const uint32_t* rank, const uint32_t* vrank, Sink sink) {
     const uint32_t n = p.host_counts[c];
     const uint32_t* list = p.list.ptr + p.host_starts[c];
     const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 8;
@@ -319,7 +343,8 @@ Error launch_bucket(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* 
     } else {
         const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(n, cap)));
         GCU_LAUNCH(dev, variant == 1 ? "wedge_cta_bucket" : "wedge_search_bucket", wedge_cta_list_kernel<Sink>, grid,
-                   kWedgeThreads, 0, d_offsets, d_targets, list, n, next, variant == 2 ? 1 : 0, split, sink);
+                   kWedgeThreads, 0, d_offsets, d_targets, list, n, next, variant == 2 ? 1 : 0, split, rank, vrank,
+                   sink);
     }
     return ok();
 }
@@ -436,7 +461,7 @@ Error plan_head(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_ta
 // warp tables below.
 template <class Sink>
 Error launch_head(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_targets, const HeadPlan& h,
-                  uint32_t* next, Sink sink) {
+                  uint32_t* next, const uint32_t* rank, const uint32_t* vrank, Sink sink) {
     const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 8;
     const int ranges[3][2] = {{kBuckets - 1, 12}, {11, 8}, {7, 0}};  // [hi, lo] buckets of variants 2, 1, 0
     for (int r = 0; r < 3; ++r) {
@@ -454,7 +479,8 @@ Error launch_head(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_
         } else {
             const unsigned grid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(n, cap)));
             GCU_LAUNCH(dev, "wedge_head_cta", wedge_head_cta_kernel<Sink>, grid, kWedgeThreads, 0, d_offsets,
-                       d_targets, items, n, h.in_off.ptr, h.in_src.ptr, next + r, variant == 2 ? 1 : 0, sink);
+                       d_targets, items, n, h.in_off.ptr, h.in_src.ptr, next + r, variant == 2 ? 1 : 0, rank, vrank,
+                       sink);
         }
     }
     return ok();
@@ -463,8 +489,9 @@ Error launch_head(DeviceImpl& dev, const uint32_t* d_offsets, const uint32_t* d_
 // Sum over DAG edges u -> v of |N+(u) ∩ N+(v)| for vertices with at least
 // min_deg out-edges. With `trace`, every valid variant of every bucket runs
 // (each into its own counter), is timed, and all must agree.
-Error count_dag(GraphImpl& g, const uint32_t* d_offsets, const uint32_t* d_targets, uint32_t m, uint32_t min_deg,
-                uint64_t* total, std::vector<TcTraceBucket>* trace) {
+Error count_dag(GraphImpl& g, const uint32_t* d_offsets, const uint32_t* d_targets, const uint32_t* d_rank,
+                const uint32_t* d_vrank, uint32_t m, uint32_t min_deg, uint64_t* total,
+                std::vector<TcTraceBucket>* trace) {
     DeviceImpl& dev = *g.dev;
     const uint32_t V = g.num_nodes;
     DegreeStats stats;
@@ -502,7 +529,7 @@ Error count_dag(GraphImpl& g, const uint32_t* d_offsets, const uint32_t* d_targe
             int variant = bucket_fixed(c);
             const int pick = p.host_choices[c];
             if (pick >= 0 && ((valid >> pick) & 1u)) variant = pick;
-            GCU_TRY(launch_bucket(dev, d_offsets, d_targets, p, c, variant, next.ptr + c, true,
+            GCU_TRY(launch_bucket(dev, d_offsets, d_targets, p, c, variant, next.ptr + c, true, d_rank, d_vrank,
                                   CountSink{totals.ptr, 0}));
             continue;
         }
@@ -510,12 +537,12 @@ Error count_dag(GraphImpl& g, const uint32_t* d_offsets, const uint32_t* d_targe
             if (!((valid >> v) & 1u)) continue;
             const int slot = c * kSchedOut + v;
             GCU_CUDA(cudaEventRecord(ev[2 * slot], dev.stream), "cudaEventRecord");
-            GCU_TRY(launch_bucket(dev, d_offsets, d_targets, p, c, v, next.ptr + slot, true,
+            GCU_TRY(launch_bucket(dev, d_offsets, d_targets, p, c, v, next.ptr + slot, true, d_rank, d_vrank,
                                   CountSink{totals.ptr + slot, 0}));
             GCU_CUDA(cudaEventRecord(ev[2 * slot + 1], dev.stream), "cudaEventRecord");
         }
     }
-    GCU_TRY(launch_head(dev, d_offsets, d_targets, head, next.ptr + kBuckets * runs + 1,
+    GCU_TRY(launch_head(dev, d_offsets, d_targets, head, next.ptr + kBuckets * runs + 1, d_rank, d_vrank,
                         CountSink{totals.ptr + head_slot, 0}));
     std::vector<unsigned long long> host(kBuckets * runs + 1);
     GCU_CUDA(cudaMemcpyAsync(host.data(), totals.ptr, sizeof(unsigned long long) * host.size(), cudaMemcpyDeviceToHost,
@@ -560,16 +587,25 @@ Error triangle_count_ex(GraphImpl& g, bool oriented, uint64_t* total, std::vecto
     if (oriented) {
         // The input is already a DAG: count over its lists as given; a
         // self-loop entry u -> u contributes |N(u)| like in the reference.
-        return count_dag(g, g.offsets.ptr, g.targets.ptr, g.num_edges, 1, total, trace);
+        return count_dag(g, g.offsets.ptr, g.targets.ptr, nullptr, nullptr, g.num_edges, 1, total, trace);
     }
     bool symmetric = false;
     GCU_TRY(graph_symmetry(g, &symmetric));
-    DeviceBuffer<uint32_t> dag_offsets, dag_targets;
+    DeviceBuffer<uint32_t> dag_offsets, dag_targets, rank, dag_rank;
     uint32_t m = 0;
-    GCU_TRY(build_dag(g, symmetric, nullptr, &dag_offsets, &dag_targets, nullptr, &m));
+    if (symmetric) {
+        // Oriented toward the higher degree class (ties by id): every
+        // out-neighbour ranks below its owner, so an owner's table can be a
+        // bitmap of the ranks below its own.
+        GCU_TRY(degree_class_order(*g.dev, g.offsets.ptr, g.num_nodes, &rank));
+        GCU_TRY(build_dag_impl(g, true, rank.ptr, nullptr, &dag_offsets, &dag_targets, nullptr, &dag_rank, &m));
+    } else {
+        GCU_TRY(build_dag(g, false, nullptr, &dag_offsets, &dag_targets, nullptr, &m));
+    }
     if (m == 0) return ok();
     // A DAG vertex needs two out-neighbours to close a triangle.
-    return count_dag(g, dag_offsets.ptr, dag_targets.ptr, m, 2, total, trace);
+    return count_dag(g, dag_offsets.ptr, dag_targets.ptr, symmetric ? dag_rank.ptr : nullptr,
+                     symmetric ? rank.ptr : nullptr, m, 2, total, trace);
 }
 
 }  // namespace
@@ -650,7 +686,8 @@ Error batch_tc_plan(GraphImpl& u, BatchTcPlan** out, std::string* tuning) {
                 if (!((valid >> v) & 1u)) continue;
                 GCU_CUDA(cudaEventRecord(ev[2 * v], dev.stream), "cudaEventRecord");
                 GCU_TRY(launch_bucket(dev, p->dag_offsets.ptr, p->dag_targets.ptr, p->buckets, c, v,
-                                      p->next.ptr + c * kSchedOut + v, false, VertexCountSink{scratch.ptr, 0}));
+                                      p->next.ptr + c * kSchedOut + v, false, nullptr, nullptr,
+                                      VertexCountSink{scratch.ptr, 0}));
                 GCU_CUDA(cudaEventRecord(ev[2 * v + 1], dev.stream), "cudaEventRecord");
             }
             GCU_TRY(dev.sync());
@@ -685,7 +722,7 @@ Error batch_tc_launch(DeviceImpl& dev, BatchTcPlan& p, unsigned long long* per_v
     for (int c = kBuckets - 1; c >= 0; --c) {
         if (p.buckets.host_counts[c] == 0) continue;
         GCU_TRY(launch_bucket(dev, p.dag_offsets.ptr, p.dag_targets.ptr, p.buckets, c, p.variant[c], p.next.ptr + c,
-                              false, VertexCountSink{per_vertex, 0}));
+                              false, nullptr, nullptr, VertexCountSink{per_vertex, 0}));
     }
     return ok();
 }

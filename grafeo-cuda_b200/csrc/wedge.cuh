@@ -84,13 +84,14 @@ __device__ __forceinline__ uint32_t sorted_find(const uint32_t* a, uint32_t n, u
 }
 
 // Walks the wedges of the out-neighbours v = list[c .. c + 31] of u (list =
-// N+(u), du entries); for every w in N+(v) that find(w) locates in N+(u) calls
+// N+(u), du entries); for every entry v -> w whose value values[entry] (the
+// target w itself, or its rank) find() locates in N+(u) calls
 // hit(pos_v, pos_w, entry_vw): positions of v and w in N+(u) and the CSR entry
 // index of v -> w. Out-neighbours with more than max_dv out-edges are skipped
 // (their edges are counted from the other end). s_excl (33 words) / s_start
 // (32 words) are per-warp scratch.
 template <class Find, class Hit>
-__device__ __forceinline__ void wedge_chunk(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
+__device__ __forceinline__ void wedge_chunk(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ values,
                                             const uint32_t* list, uint32_t du, uint32_t c, uint32_t* s_excl,
                                             uint32_t* s_start, uint32_t max_dv, Find find, Hit hit) {
     const unsigned lane = lane_id();
@@ -121,7 +122,7 @@ __device__ __forceinline__ void wedge_chunk(const uint32_t* __restrict__ offsets
             next = s_excl[lo + 1];
         }
         const uint32_t entry = start + (k - first);
-        const uint32_t p = find(targets[entry]);
+        const uint32_t p = find(values[entry]);
         if (p != kNotFound) hit(c + lo, p, entry);
     }
 }
@@ -146,6 +147,70 @@ constexpr uint32_t kCtaMaxDeg = 2048;   // CTA kernel: hash table up to this len
 constexpr uint32_t kCtaBits = 12;
 constexpr uint32_t kCtaSlots = 1u << kCtaBits;
 constexpr uint32_t kVertexBatch = 8;    // vertices fetched per warp at a time
+
+// The lookup structure of a CTA item whose owner x has the out-list
+// entries [s, s + d):
+//  kBitmap: with ranks (a DAG oriented by a vertex order, rank[entry] = the
+//    position of the entry's target in that order, every out-neighbour
+//    ranked below its owner), a bitmap of the ranks below vrank[x] when it
+//    fits the shared array: one bit test per probe, no probe loop, no hash;
+//  kHash: a hash table of the values probed (ranks, or the targets);
+//  kSearch: binary search of the sorted targets in global memory.
+enum : int { kSearch = 0, kHash = 1, kBitmap = 2 };
+struct CtaTable {
+    int kind;
+    uint32_t bits;             // kHash: log2 of the slots
+    uint32_t limit;            // kBitmap: ranks below this are covered
+    const uint32_t* values;    // what the probes look up (ranks or targets)
+};
+
+template <bool kPos>
+__device__ __forceinline__ CtaTable build_cta_table(uint32_t* s_keys, uint32_t* pos,
+                                                    const uint32_t* __restrict__ targets,
+                                                    const uint32_t* __restrict__ rank,
+                                                    const uint32_t* __restrict__ vrank, uint32_t x, uint32_t s,
+                                                    uint32_t d, int search) {
+    CtaTable t{kSearch, 0, 0, targets};
+    if (search) return t;
+    if (!kPos && rank) {
+        t.values = rank;
+        const uint32_t r = vrank[x];
+        if (r <= kCtaSlots * 32) {
+            t.kind = kBitmap;
+            t.limit = r;
+            for (uint32_t k = threadIdx.x; k < (r + 31) / 32; k += kWedgeThreads) s_keys[k] = 0;
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < d; k += kWedgeThreads) {
+                const uint32_t w = rank[s + k];
+                if (w < r) atomicOr(s_keys + (w >> 5), 1u << (w & 31));
+            }
+            __syncthreads();
+            return t;
+        }
+    }
+    if (d <= kCtaMaxDeg) {
+        t.kind = kHash;
+        t.bits = table_bits(d, kCtaBits);
+        for (uint32_t k = threadIdx.x; k < (1u << t.bits); k += kWedgeThreads) s_keys[k] = kEmptyKey;
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < d; k += kWedgeThreads)
+            hash_insert<kPos>(s_keys, pos, t.bits, t.values[s + k], k);
+        __syncthreads();
+        return t;
+    }
+    t.values = targets;
+    return t;
+}
+
+// Position of the probed value w in the owner's list (kNotFound if absent; 0
+// for any hit in a bitmap, which keeps no positions).
+template <bool kPos>
+__device__ __forceinline__ uint32_t cta_find(const CtaTable& t, const uint32_t* s_keys, const uint32_t* pos,
+                                             const uint32_t* sorted_list, uint32_t d, uint32_t w) {
+    if (t.kind == kBitmap) return (w < t.limit && ((s_keys[w >> 5] >> (w & 31)) & 1u)) ? 0u : kNotFound;
+    if (t.kind == kHash) return hash_find<kPos>(s_keys, pos, t.bits, w);
+    return sorted_find(sorted_list, d, w);
+}
 
 // A Sink receives every triangle: hit(row_base, pos_v, pos_w, entry_vw) with
 // row_base = offsets[u] (so row_base + pos_v is the entry u -> v) and
@@ -310,15 +375,17 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_warp_list_kernel(const ui
     sink.finish();
 }
 
-// CTA per listed vertex: a shared hash table (out-lists of at most
+// CTA per listed vertex: a shared bitmap of ranks (`rank` given, the owner's
+// rank within the shared array), a shared hash table (out-lists of at most
 // kCtaMaxDeg entries, unless `search`) or binary search of the out-list in
-// global memory.
+// global memory (build_cta_table).
 template <class Sink>
 __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_list_kernel(const uint32_t* __restrict__ offsets,
                                                                        const uint32_t* __restrict__ targets,
                                                                        const uint32_t* __restrict__ list, uint32_t n,
                                                                        uint32_t* __restrict__ next, int search,
-                                                                       bool split, Sink sink) {
+                                                                       bool split, const uint32_t* __restrict__ rank,
+                                                                       const uint32_t* __restrict__ vrank, Sink sink) {
     constexpr bool kPos = Sink::kNeedsPos;
     __shared__ uint32_t s_keys[kCtaSlots];
     __shared__ uint32_t s_pos[kPos ? kCtaSlots : 1];
@@ -338,21 +405,12 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_cta_list_kernel(const uin
         const uint32_t u = list[h];
         const uint32_t s = offsets[u], du = offsets[u + 1] - s;
         const uint32_t* ulist = targets + s;
-        const bool use_table = !search && du <= kCtaMaxDeg;
-        const uint32_t bits = use_table ? table_bits(du, kCtaBits) : 0;
-        if (use_table) {
-            for (uint32_t k = threadIdx.x; k < (1u << bits); k += kWedgeThreads) s_keys[k] = kEmptyKey;
-            __syncthreads();
-            for (uint32_t k = threadIdx.x; k < du; k += kWedgeThreads) hash_insert<kPos>(s_keys, pos, bits, ulist[k], k);
-            __syncthreads();
-        }
+        const CtaTable tab = build_cta_table<kPos>(s_keys, pos, targets, rank, vrank, u, s, du, search);
         const uint32_t max_dv = split && du >= 2 ? du : 0xFFFFFFFFu;
         for (uint32_t c = next_chunk(&s_chunk); c < du; c = next_chunk(&s_chunk))
             wedge_chunk(
-                offsets, targets, ulist, du, c, s_excl[warp], s_start[warp], max_dv,
-                [&](uint32_t w) {
-                    return use_table ? hash_find<kPos>(s_keys, pos, bits, w) : sorted_find(ulist, du, w);
-                },
+                offsets, tab.values, ulist, du, c, s_excl[warp], s_start[warp], max_dv,
+                [&](uint32_t w) { return cta_find<kPos>(tab, s_keys, pos, ulist, du, w); },
                 [&](uint32_t pv, uint32_t pw, uint32_t evw) { sink.hit(s, pv, pw, evw); });
         sink.end_vertex(u);
         __syncthreads();  // the table and s_item are reused by the next list
@@ -430,7 +488,7 @@ template <class Sink>
 __global__ void __launch_bounds__(kWedgeThreads) wedge_head_cta_kernel(
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, const uint2* __restrict__ items,
     uint32_t n, const uint32_t* __restrict__ in_off, const uint32_t* __restrict__ in_src, uint32_t* __restrict__ next,
-    int search, Sink sink) {
+    int search, const uint32_t* __restrict__ rank, const uint32_t* __restrict__ vrank, Sink sink) {
     __shared__ uint32_t s_keys[kCtaSlots];
     __shared__ uint32_t s_excl[kWedgeWarps][33];
     __shared__ uint32_t s_start[kWedgeWarps][32];
@@ -447,24 +505,14 @@ __global__ void __launch_bounds__(kWedgeThreads) wedge_head_cta_kernel(
         const uint2 item = items[h];
         const uint32_t s = offsets[item.x], dv = offsets[item.x + 1] - s;
         const uint32_t* vlist = targets + s;
-        const bool use_table = !search && dv <= kCtaMaxDeg;
-        const uint32_t bits = use_table ? table_bits(dv, kCtaBits) : 0;
-        if (use_table) {
-            for (uint32_t k = threadIdx.x; k < (1u << bits); k += kWedgeThreads) s_keys[k] = kEmptyKey;
-            __syncthreads();
-            for (uint32_t k = threadIdx.x; k < dv; k += kWedgeThreads)
-                hash_insert<false>(s_keys, nullptr, bits, vlist[k], k);
-            __syncthreads();
-        }
+        const CtaTable tab = build_cta_table<false>(s_keys, nullptr, targets, rank, vrank, item.x, s, dv, search);
         const uint32_t* tails;
         uint32_t count;
         head_slice(item, in_off, in_src, kHeadCtaSlice, tails, count);
         for (uint32_t c = next_chunk(&s_chunk); c < count; c = next_chunk(&s_chunk))
             wedge_chunk(
-                offsets, targets, tails, count, c, s_excl[warp], s_start[warp], 0xFFFFFFFFu,
-                [&](uint32_t w) {
-                    return use_table ? hash_find<false>(s_keys, nullptr, bits, w) : sorted_find(vlist, dv, w);
-                },
+                offsets, tab.values, tails, count, c, s_excl[warp], s_start[warp], 0xFFFFFFFFu,
+                [&](uint32_t w) { return cta_find<false>(tab, s_keys, nullptr, vlist, dv, w); },
                 [&](uint32_t pu, uint32_t pw, uint32_t e) { sink.hit(s, pu, pw, e); });
         __syncthreads();  // the table and s_item are reused by the next item
     }
