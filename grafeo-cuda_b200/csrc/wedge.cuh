@@ -1,9 +1,11 @@
-// Wedge enumeration over a DAG CSR with shared-memory hash tables.
+// Wedge enumeration over a DAG CSR with shared-memory tables.
 //
 // Shared by triangle counting and k-truss support counting. For a vertex u
-// with out-list N+(u), the keys of N+(u) go into an open-addressing hash table
-// in shared memory (multiplicative hashing, linear probing, load <= 1/2), then
-// every wedge (v, w), v in N+(u), w in N+(v), is probed: a hit is a triangle
+// with out-list N+(u), the keys of N+(u) go into a table in shared memory: an
+// open-addressing hash table (multiplicative hashing, linear probing, load
+// <= 1/2, <= 1/4 where the slots allow) or, when the DAG is oriented by a
+// vertex rank and u's rank fits, a bitmap of the ranks below u's. Then every
+// wedge (v, w), v in N+(u), w in N+(v), is probed: a hit is a triangle
 // {u, v, w}. The wedges of up to 32 v's at a time are spread evenly over the
 // lanes of a warp by a warp scan of the d+(v) (a load-balanced search), so the
 // reads of the N+(v) lists are coalesced and no lane idles on short lists.
