@@ -5,6 +5,7 @@
 // O(V) loop on one GPU thread. Three passes: per-tile sums, a scan of the tile
 // sums in one block, then the per-tile scan with its carry-in. Each tile is
 // 1024 threads x 8 items; the input is read twice and the output written once.
+// Inputs of one tile take a single launch.
 #include "device_common.cuh"
 #include "gcu_internal.h"
 
@@ -89,9 +90,48 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const uint32_t
     }
 }
 
+// One tile (n <= kScanTile): the whole scan in one launch, the total in
+// out[n]. Every thread reads its items before it writes them, so in == out
+// is fine.
+__global__ void __launch_bounds__(kScanThreads) scan_one_tile_kernel(const uint32_t* __restrict__ in, uint32_t n,
+                                                                    uint32_t* __restrict__ out) {
+    __shared__ uint32_t warp_tot[32];
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    uint32_t v[kScanItems];
+    uint32_t local = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t i = threadIdx.x * kScanItems + k;
+        v[k] = i < n ? in[i] : 0;
+        local += v[k];
+    }
+    const uint32_t inc = warp_inclusive_scan(local);
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = warp_tot[lane];
+        warp_tot[lane] = warp_inclusive_scan(w) - w;
+    }
+    __syncthreads();
+    uint32_t run = warp_tot[warp] + inc - local;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        const uint32_t i = threadIdx.x * kScanItems + k;
+        if (i < n) out[i] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == kScanThreads - 1) out[n] = run;
+}
+
 Error exclusive_scan_u32(DeviceImpl& dev, const uint32_t* d_in, uint32_t* d_out, uint64_t n) {
     if (n == 0) {
         GCU_CUDA(cudaMemsetAsync(d_out, 0, sizeof(uint32_t), dev.stream), "memset");
+        return ok();
+    }
+    if (n <= static_cast<uint64_t>(kScanTile)) {
+        // Small inputs (BFS frontiers, per-round peel lists): one launch.
+        GCU_LAUNCH(dev, "scan_one_tile", scan_one_tile_kernel, 1, kScanThreads, 0, d_in, static_cast<uint32_t>(n),
+                   d_out);
         return ok();
     }
     const uint64_t tiles = ceil_div_u64(n, kScanTile);
