@@ -367,8 +367,6 @@ GCU_API gcu_status gcu_graph_from_csr(gcu_device* dev, const uint32_t* offsets, 
                                 std::to_string(n_targets) + " entries"));
     }
 
-    WallTimer wall;
-    (void)wall;
     auto g = std::make_unique<GraphImpl>();
     g->dev = dev->impl;
     DeviceImpl& d = *g->dev;
