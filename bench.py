@@ -62,6 +62,10 @@ def parse_args():
                          "R-MAT 24 (directed PageRank with 3%% dangling vertices and its error, truss "
                          "decomposition, BFS and triangles with the learned schedule against the fixed rules); "
                          "one JSON document")
+    ap.add_argument("--bfs-breakdown", action="store_true",
+                    help="instead of the headline: BFS from 16 random sources on R-MAT 22 and Erdos-Renyi 2^22, "
+                         "wall time per search against the sum of its kernels' CUDA-event times (what the per-level "
+                         "host round trips cost), per kernel; one JSON document")
     return ap.parse_args()
 
 
@@ -608,10 +612,53 @@ def run_reference(args, d: Dist) -> dict | None:
     }
 
 
+def run_bfs_breakdown() -> dict:
+    """Device time of 16 searches (CUDA events around the run) against the sum
+    of their kernels' own event times, and the per-kernel split."""
+    import grafeo_cuda as G
+
+    dev = G.GpuDevice(0)
+    out = {"bfs_breakdown": "16 random sources per graph; ms per search", "device": dev.name}
+    graphs = (
+        ("rmat22", lambda: G.GpuGraph.generate_rmat(dev, 22, EDGE_FACTOR, *RMAT_ABC, seed=2)),
+        ("er22", lambda: G.GpuGraph.generate_erdos_renyi(dev, 1 << 22, 16 << 22, seed=3)),
+    )
+    for name, make in graphs:
+        g = make()
+        sources = [int(x) for x in np.random.default_rng(1).integers(0, g.num_nodes, 16)]
+        for s in sources[:3]:
+            g.bfs_array(s, copy_result=False)
+        dev.timer_start()
+        for s in sources:
+            g.bfs_array(s, copy_result=False)
+        wall_ms = dev.timer_stop()
+        dev.set_kernel_timing(True)
+        dev.reset_stats()
+        depth = 0
+        for s in sources:
+            depth += g.bfs_array(s, copy_result=False)["max_depth"]
+        stats = dev.kernel_stats()
+        dev.set_kernel_timing(False)
+        kernel_ms = sum(v[1] for v in stats.values())
+        out[name] = {
+            "ms_per_search": round(wall_ms / len(sources), 4),
+            "kernel_ms_per_search": round(kernel_ms / len(sources), 4),
+            "kernel_share": round(kernel_ms / wall_ms, 3) if wall_ms else None,
+            "levels_per_search": depth / len(sources),
+            "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)}
+                        for k, v in sorted(stats.items(), key=lambda kv: -kv[1][1])},
+        }
+        del g
+    return out
+
+
 def main():
     args = parse_args()
     if args.suite:
         print(json.dumps(run_suite(args)), flush=True)
+        return
+    if args.bfs_breakdown:
+        print(json.dumps(run_bfs_breakdown()), flush=True)
         return
     d = Dist()
     try:
