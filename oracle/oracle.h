@@ -90,6 +90,46 @@ size_t orc_from_edge_pairs_oriented(const uint32_t* pairs, size_t n_pairs, uint3
 /* Number of OpenMP threads the oracle uses. */
 int orc_num_threads(void);
 
+/* ---- at scale (oracle_scale.c): parallel restatements for the large
+ * configurations; see that file's header for what each restates. */
+
+/* Symmetric, loop-free, deduplicated CSR of an R-MAT graph: edge_factor << scale
+ * pairs, pair i choosing one quadrant per level (a, b, c, rest) from SplitMix64
+ * draws i * scale + level of the stream seeded by `seed`. `targets` holds at
+ * least 2 * (edge_factor << scale) entries; returns the entry count. */
+size_t orc_generate_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed,
+                         uint32_t* offsets, uint32_t* targets);
+
+/* The same for Erdos-Renyi G(n, num_pairs): pair i = draws 2i and 2i + 1
+ * mapped onto [0, n). `targets` holds at least 2 * num_pairs entries. */
+size_t orc_generate_erdos_renyi(uint32_t n, uint64_t num_pairs, uint64_t seed, uint32_t* offsets,
+                                uint32_t* targets);
+
+/* orc_transpose by a parallel radix sort (same output). */
+size_t orc_transpose_sorted(const uint32_t* offsets, const uint32_t* targets, uint32_t n, uint32_t* t_offsets,
+                            uint32_t* t_targets);
+
+/* support[j] = triangles through the edge of entry j; -1 unless the CSR is
+ * simple (no self-loops or repeated entries) and symmetric. */
+int orc_edge_support(const uint32_t* offsets, const uint32_t* targets, uint32_t n, uint32_t* support);
+
+/* orc_k_truss on a simple symmetric CSR by incremental peeling (same edges,
+ * same round count). support0 (optional) is orc_edge_support's output, to
+ * share it across several k. Returns the edge count, or SIZE_MAX when the
+ * CSR is not simple and symmetric. */
+size_t orc_k_truss_peel(const uint32_t* offsets, const uint32_t* targets, uint32_t n, uint32_t k,
+                        const uint32_t* support0, uint32_t* out, uint32_t* iterations);
+
+/* Truss decomposition by the same peeling continued level by level: the
+ * trussness of every entry's edge (2 for edges in no triangle), the largest
+ * k with a non-empty k-truss, and the number of synchronous rounds (a round
+ * that removes nothing ends its level and is counted). -1 unless simple and
+ * symmetric. */
+int orc_truss_decomposition_peel(const uint32_t* offsets, const uint32_t* targets, uint32_t n,
+                                 const uint32_t* support0, uint32_t* trussness, uint32_t* max_trussness,
+                                 uint32_t* rounds);
+
+
 #ifdef __cplusplus
 }
 #endif

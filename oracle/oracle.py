@@ -20,8 +20,8 @@ u32p = C.POINTER(C.c_uint32)
 
 
 def build(force: bool = False) -> str:
-    src = os.path.join(HERE, "oracle.c")
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(src):
+    newest = max(os.path.getmtime(os.path.join(HERE, f)) for f in ("oracle.c", "oracle_scale.c", "oracle.h"))
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < newest:
         subprocess.run(["make", "-B", "-C", HERE], check=True, capture_output=True)
     return LIB_PATH
 
@@ -56,6 +56,19 @@ def _load() -> C.CDLL:
     lib.orc_from_edge_pairs_oriented.argtypes = [u32p, C.c_size_t, C.c_uint32, u32p, u32p]
     lib.orc_num_threads.restype = C.c_int
     lib.orc_num_threads.argtypes = []
+    lib.orc_generate_rmat.restype = C.c_size_t
+    lib.orc_generate_rmat.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                      u32p, u32p]
+    lib.orc_generate_erdos_renyi.restype = C.c_size_t
+    lib.orc_generate_erdos_renyi.argtypes = [C.c_uint32, C.c_uint64, C.c_uint64, u32p, u32p]
+    lib.orc_transpose_sorted.restype = C.c_size_t
+    lib.orc_transpose_sorted.argtypes = [u32p, u32p, C.c_uint32, u32p, u32p]
+    lib.orc_edge_support.restype = C.c_int
+    lib.orc_edge_support.argtypes = [u32p, u32p, C.c_uint32, u32p]
+    lib.orc_k_truss_peel.restype = C.c_size_t
+    lib.orc_k_truss_peel.argtypes = [u32p, u32p, C.c_uint32, C.c_uint32, u32p, u32p, u32p]
+    lib.orc_truss_decomposition_peel.restype = C.c_int
+    lib.orc_truss_decomposition_peel.argtypes = [u32p, u32p, C.c_uint32, u32p, u32p, u32p, u32p]
     return lib
 
 
@@ -130,11 +143,21 @@ def transpose(offsets, targets):
     return to, tt[: len(t)]
 
 
+def transpose_sorted(offsets, targets):
+    """transpose() by the parallel radix sort (for graphs at scale)."""
+    o, t = _u32(offsets), _u32(targets)
+    n = len(o) - 1
+    to = np.zeros(n + 1, dtype=np.uint32)
+    tt = np.zeros(max(len(t), 1), dtype=np.uint32)
+    lib().orc_transpose_sorted(_p(o), _p(t), n, _p(to), _p(tt))
+    return to, tt[: len(t)]
+
+
 def pagerank_directed(offsets, targets, damping=0.85, max_iterations=100, tolerance=1e-6, rule="l1",
                       tele=None) -> dict:
     """PageRank of the directed graph whose out-edges are the CSR lists."""
     o = _u32(offsets)
-    to, tt = transpose(offsets, targets)
+    to, tt = transpose_sorted(offsets, targets) if len(o) > (1 << 16) else transpose(offsets, targets)
     return pagerank(to, tt, damping, max_iterations, tolerance, rule, out_degree=np.diff(o), tele=tele)
 
 
@@ -195,3 +218,64 @@ def from_edge_pairs_oriented(edges, num_nodes: int):
     if m == C.c_size_t(-1).value:
         raise ValueError("edge references a node >= num_nodes")
     return offsets, targets[:m]
+
+
+# ---------------------------------------------------------------- at scale (oracle_scale.c)
+
+
+class Csr:
+    """A CSR built by the oracle's generators (same fields as the library's)."""
+
+    def __init__(self, offsets: np.ndarray, targets: np.ndarray):
+        self.offsets, self.targets = offsets, targets
+        self.num_nodes, self.num_edges = len(offsets) - 1, len(targets)
+
+
+def generate_rmat(scale: int, edge_factor: int, a: float, b: float, c: float, seed: int) -> Csr:
+    n = 1 << scale
+    offsets = np.zeros(n + 1, dtype=np.uint32)
+    targets = np.empty(max(2 * (edge_factor << scale), 1), dtype=np.uint32)
+    m = lib().orc_generate_rmat(scale, edge_factor, a, b, c, seed, _p(offsets), _p(targets))
+    if m == C.c_size_t(-1).value:
+        raise ValueError("R-MAT scale must be in 1..=31")
+    return Csr(offsets, targets[:m].copy())
+
+
+def generate_erdos_renyi(n: int, num_pairs: int, seed: int) -> Csr:
+    offsets = np.zeros(n + 1, dtype=np.uint32)
+    targets = np.empty(max(2 * num_pairs, 1), dtype=np.uint32)
+    m = lib().orc_generate_erdos_renyi(n, num_pairs, seed, _p(offsets), _p(targets))
+    return Csr(offsets, targets[:m].copy())
+
+
+def edge_support(offsets, targets) -> np.ndarray:
+    """Triangles through the edge of every entry (simple symmetric CSR)."""
+    o, t = _u32(offsets), _u32(targets)
+    s = np.zeros(max(len(t), 1), dtype=np.uint32)
+    if lib().orc_edge_support(_p(o), _p(t), len(o) - 1, _p(s)) != 0:
+        raise ValueError("edge_support needs a simple symmetric CSR")
+    return s[: len(t)]
+
+
+def k_truss_peel(offsets, targets, k: int, support=None) -> dict:
+    """k_truss() for a simple symmetric CSR by incremental peeling."""
+    o, t = _u32(offsets), _u32(targets)
+    out = np.zeros(max(len(t), 2), dtype=np.uint32)
+    it = C.c_uint32()
+    sp = None if support is None else _p(_u32(support))
+    m = lib().orc_k_truss_peel(_p(o), _p(t), len(o) - 1, int(k), sp, _p(out), C.byref(it))
+    if m == C.c_size_t(-1).value:
+        raise ValueError("k_truss_peel needs a simple symmetric CSR")
+    return {"edges": out[: 2 * m].reshape(m, 2), "iterations": int(it.value)}
+
+
+def truss_decomposition_peel(offsets, targets, support=None) -> dict:
+    """truss_decomposition() for a simple symmetric CSR by peeling, with the
+    synchronous round count."""
+    o, t = _u32(offsets), _u32(targets)
+    tr = np.zeros(max(len(t), 1), dtype=np.uint32)
+    top, rounds = C.c_uint32(), C.c_uint32()
+    sp = None if support is None else _p(_u32(support))
+    if lib().orc_truss_decomposition_peel(_p(o), _p(t), len(o) - 1, sp, _p(tr), C.byref(top), C.byref(rounds)) != 0:
+        raise ValueError("truss_decomposition_peel needs a simple symmetric CSR")
+    return {"trussness": tr[: len(t)], "max_trussness": int(top.value), "rounds": int(rounds.value)}

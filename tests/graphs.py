@@ -154,6 +154,18 @@ def symmetric_csr(n: int, src: np.ndarray, dst: np.ndarray):
     return np.cumsum(offsets, dtype=np.uint64).astype(np.uint32), (keys & np.uint64(0xFFFFFFFF)).astype(np.uint32)
 
 
+def rmat_pairs(scale: int, edge_factor: int, a: float, b: float, c: float, seed: int):
+    """R-MAT pairs: pair i picks one quadrant per level (top bit first) from
+    draw i * scale + level: below a (0, 0), below a + b (0, 1), below
+    a + b + c (1, 0), else (1, 1)."""
+    m = edge_factor << scale
+    u = _unit(_stream(_state(seed), np.arange(m * scale, dtype=np.uint64))).reshape(m, scale)
+    row = (u >= a + b).astype(np.uint32)
+    col = (((u >= a) & (u < a + b)) | (u >= a + b + c)).astype(np.uint32)
+    weights = (np.uint32(1) << np.arange(scale - 1, -1, -1, dtype=np.uint32))
+    return (row * weights).sum(axis=1).astype(np.uint32), (col * weights).sum(axis=1).astype(np.uint32)
+
+
 def grid_pairs(width: int, height: int, drop: float, seed: int):
     horizontal = height * (width - 1)
     e = np.arange(horizontal + (height - 1) * width, dtype=np.uint64)

@@ -199,3 +199,113 @@ def test_oracle_k_truss_round_semantics_on_self_loops():
     # Edge 2-3 is kept in round 1 (self-loops at 2 and 3 count as common
     # neighbours), loses the self-loops in round 1, and goes in round 2.
     assert r["iterations"] == 3
+
+
+# ---------------------------------------------------------------- the oracle at scale (oracle_scale.c)
+
+
+def _simple(g) -> bool:
+    o, t = csr(g)
+    src = np.repeat(np.arange(g["num_nodes"]), np.diff(o))
+    return not np.any(src == t)
+
+
+@pytest.mark.parametrize("scale,seed", [(1, 1), (6, 7), (11, 2), (14, 1)])
+def test_oracle_rmat_generator_matches_library_and_numpy(scale, seed):
+    """The oracle's radix-sort R-MAT builder equals the library's host
+    generator (bucket sort) entry for entry, and the numpy restatement of the
+    pair draws in tests/graphs.py."""
+    import grafeo_cuda as G
+
+    a = O.generate_rmat(scale, 16, 0.57, 0.19, 0.19, seed)
+    b = G.generate_rmat(scale, 16, 0.57, 0.19, 0.19, seed=seed)
+    assert np.array_equal(a.offsets, b.offsets) and np.array_equal(a.targets, b.targets)
+    if scale <= 11:
+        s, d = graphs.rmat_pairs(scale, 16, 0.57, 0.19, 0.19, seed)
+        o, t = O.from_edge_pairs(np.stack([s, d], axis=1)[s != d], 1 << scale, True)
+        assert np.array_equal(a.offsets, o) and np.array_equal(a.targets, t)
+
+
+@pytest.mark.parametrize("n,pairs,seed", [(0, 0, 1), (1, 5, 1), (1000, 16000, 3), (70000, 1 << 20, 3)])
+def test_oracle_erdos_renyi_generator_matches_library(n, pairs, seed):
+    import grafeo_cuda as G
+
+    a = O.generate_erdos_renyi(n, pairs, seed)
+    b = G.generate_erdos_renyi(n, pairs, seed=seed)
+    assert np.array_equal(a.offsets, b.offsets) and np.array_equal(a.targets, b.targets)
+
+
+def test_oracle_sorted_transpose_matches_serial_transpose():
+    rng = np.random.default_rng(5)
+    for n in (1, 7, 300, 5000):
+        pairs = rng.integers(0, n, size=(4 * n, 2))
+        o, t = O.from_edge_pairs(pairs, n, False)
+        x, y = O.transpose(o, t), O.transpose_sorted(o, t)
+        assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+    c = O.generate_rmat(13, 16, 0.57, 0.19, 0.19, 4)
+    x, y = O.transpose(c.offsets, c.targets), O.transpose_sorted(c.offsets, c.targets)
+    assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+
+
+def test_oracle_edge_support_counts_triangles(golden_graphs):
+    for g in golden_graphs:
+        if not _simple(g):
+            continue
+        o, t = csr(g)
+        s = O.edge_support(o, t)
+        assert int(s.sum()) == 6 * g["triangles"], g["name"]
+    c = O.generate_rmat(14, 16, 0.57, 0.19, 0.19, 1)
+    assert int(O.edge_support(c.offsets, c.targets).sum()) == 6 * O.triangle_count(c.offsets, c.targets)
+    with pytest.raises(ValueError):
+        O.edge_support([0, 1, 1], [1])  # not symmetric
+    with pytest.raises(ValueError):
+        O.edge_support([0, 1], [0])  # self-loop
+
+
+def test_oracle_peeling_k_truss_matches_full_recomputation(golden_graphs):
+    """The incremental peel gives orc_k_truss's edges and round counts (the
+    reference's round rule) on the catalog, the property-test graphs without
+    self-loops and random R-MAT / Erdos-Renyi graphs."""
+    cases = [csr(g) for g in golden_graphs if _simple(g)]
+    for scale, seed in ((9, 1), (11, 3), (12, 2)):
+        c = O.generate_rmat(scale, 16, 0.57, 0.19, 0.19, seed)
+        cases.append((c.offsets, c.targets))
+    c = O.generate_erdos_renyi(3000, 3000 * 12, 9)
+    cases.append((c.offsets, c.targets))
+    for o, t in cases:
+        sup = O.edge_support(o, t) if len(t) else None
+        for k in (2, 3, 4, 5, 6, 8, 11):
+            a, b = O.k_truss(o, t, k), O.k_truss_peel(o, t, k, sup)
+            assert np.array_equal(a["edges"], b["edges"]), k
+            assert a["iterations"] == b["iterations"], k
+
+
+def test_oracle_peeling_decomposition_matches_definition_and_round_rule(golden_graphs):
+    """Trussness from the peel equals the definition-based decomposition;
+    rounds equal the host restatement of the device's level-by-level rule."""
+    import random
+
+    import test_peel_frontier as PF
+
+    for g in golden_graphs:
+        if not _simple(g):
+            continue
+        o, t = csr(g)
+        a, b = O.truss_decomposition(o, t), O.truss_decomposition_peel(o, t)
+        assert np.array_equal(a["trussness"], b["trussness"]) and a["max_trussness"] == b["max_trussness"], g["name"]
+    rng = random.Random(11)
+    for _ in range(60):
+        n = rng.randint(2, 30)
+        pairs = [(rng.randrange(n), rng.randrange(n)) for _ in range(rng.randint(0, n * 6))]
+        pairs = [(x, y) for x, y in pairs if x != y]
+        o, t = O.from_edge_pairs(pairs, n, True)
+        rounds, top, truss = PF.decomposition(n, pairs, True)
+        b = O.truss_decomposition_peel(o, t)
+        assert b["rounds"] == rounds and b["max_trussness"] == top, pairs
+        src = np.repeat(np.arange(n), np.diff(o))
+        edges = sorted({(min(x, y), max(x, y)) for x, y in pairs})
+        by_edge = dict(zip(edges, truss))
+        assert [by_edge[(min(x, y), max(x, y))] for x, y in zip(src, t)] == b["trussness"].tolist(), pairs
+    c = O.generate_rmat(12, 16, 0.57, 0.19, 0.19, 6)
+    a, b = O.truss_decomposition(c.offsets, c.targets), O.truss_decomposition_peel(c.offsets, c.targets)
+    assert np.array_equal(a["trussness"], b["trussness"]) and a["max_trussness"] == b["max_trussness"]
