@@ -1,26 +1,43 @@
 #!/usr/bin/env python
-"""Benchmark of the four graph hot paths on R-MAT scale 22 (seed 2).
+"""Benchmark of the four graph hot paths; headline on R-MAT scale 24 (seed 5).
 
 Headline (`metric`/`value`): PageRank iteration throughput in GB/s of
-algorithmic traffic, B = 4E + 12V + 4 bytes per iteration (offsets, targets,
-one read of the contribution vector and one write of the ranks), on R-MAT
-scale 22 (4,194,304 vertices, edge factor 16, a=0.57 b=0.19 c=0.19, seed 2),
-50 iterations at damping 0.85 per step. The same JSON line carries BFS
-(GTEPS from 64 seeded random non-isolated sources), triangle counting
-(edges/s) and k-truss (edges/s, k = 3..8) on the same graph.
+algorithmic traffic, B = 4E + 12V + 4 bytes per iteration (offsets and
+targets of the pulled in-CSR, one read of the contribution vector and one
+write of the ranks), on the large skewed configuration: R-MAT scale 24
+(16,777,216 vertices, edge factor 16, a=0.57 b=0.19 c=0.19, seed 5),
+symmetrised and deduplicated, then a directed copy in which a seeded
+uniform 3 % of the vertices lose their out-edges (dangling). One step is one
+PageRank run at damping 0.85 to an L1 change below 1e-7 (at most 100
+iterations): FP32 row sums with compensation, FP64 residual and dangling
+mass. Its L1 and Linf error against the FP64 oracle at the same iteration
+count ride along (computed outside the timed region).
 
   value  device time (CUDA events on the library's stream) with the CSR
-         already resident in HBM; inputs (0.53 GB CSR) are larger than L2.
+         already resident in HBM (2 GB, larger than L2); the transpose plan
+         is built once per graph, before the timed region.
   e2e    the same metric through the public API with host buffers: every step
-         copies the CSR from pinned host memory (GpuGraph.from_csr, which also
-         validates it), runs pagerank and copies the ranks back.
-  roofline  the dominant kernel (one launch = one iteration) against the measured HBM
-         copy bandwidth.
-  cpu_baseline  the oracle's OpenMP FP64 PageRank on this host's cores, on a
-         bounded sample of the same workload.
+         copies the directed CSR from pinned host memory (GpuGraph.from_csr,
+         which validates it), builds the transpose plan, runs PageRank and
+         copies the ranks back; wall time.
+  roofline  the dominant kernel (one launch = one iteration) against the
+         measured HBM copy bandwidth.
+  cpu_baseline  the oracle's OpenMP FP64 PageRank on this host's cores: the
+         same iteration count on the same graph (the run the error is taken
+         from).
+  harness  one record per algorithm and graph in the reference's
+         GpuBenchmarkResult layout (crates/grafeo-cuda-algos/src/harness.rs:14-52),
+         with every run's kernel time, the median and the best.
+  algorithms  BFS (64 seeded non-isolated sources), triangle counting and the
+         truss decomposition on the symmetric R-MAT 24 graph, with the learned
+         schedule against the fixed rules; PageRank, BFS, triangles and the
+         k-truss sweep k = 3..8 on R-MAT 22 (seed 2) and Erdos-Renyi 2^22
+         (seed 3).
 
 `--impl reference` times the reference's CPU implementation of the path (the
-oracle port; Grafeo's own Rust crate cannot be built here) on the same metric.
+oracle port; Grafeo's own Rust crate cannot be built here) on the same metric
+and configuration; its graph comes from the oracle's own generator, so it
+loads nothing of this project's library.
 
 Multi-GPU (torchrun): one process per GPU, each a full replica of the graph
 running its own PageRank (no data-path collective; weak scaling); value is the
@@ -31,6 +48,8 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import platform
+import socket
 import statistics
 import subprocess
 import sys
@@ -42,11 +61,19 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "grafeo-cuda_b200"))
 sys.path.insert(0, ROOT)
 
-SCALE, EDGE_FACTOR, SEED = 22, 16, 2
+EDGE_FACTOR = 16
 RMAT_ABC = (0.57, 0.19, 0.19)
 DAMPING = 0.85
+# The headline configuration: R-MAT 24, seed 5, directed copy with 3 % dangling vertices.
+SCALE, SEED = 24, 5
+DANGLING = 0.03
+TOLERANCE = 1e-7
+MAX_ITERATIONS = 100
+# The secondary configurations (R-MAT 22 seed 2, Erdos-Renyi 2^22 seed 3).
 PR_ITERATIONS = 50
 BFS_SOURCES = 64
+RUNS = 5
+METRIC = "PageRank iteration GB/s (algorithmic bytes 4E+12V+4 per iteration, E = pulled in-CSR entries)"
 
 
 def parse_args():
@@ -56,16 +83,12 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--scale", type=int, default=SCALE)
-    ap.add_argument("--no-secondary", action="store_true", help="skip BFS/TC/k-truss lines")
-    ap.add_argument("--suite", action="store_true",
-                    help="instead of the headline: all four algorithms on R-MAT 22 and Erdos-Renyi 2^22, and "
-                         "R-MAT 24 (directed PageRank with 3%% dangling vertices and its error, truss "
-                         "decomposition, BFS and triangles with the learned schedule against the fixed rules); "
-                         "one JSON document")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the algorithms block and the harness records")
+    ap.add_argument("--save", metavar="DIR", help="also write every harness record to DIR/gpu_<algorithm>_<dataset>.json")
     ap.add_argument("--bfs-breakdown", action="store_true",
                     help="instead of the headline: BFS from 16 random sources on R-MAT 22 and Erdos-Renyi 2^22, "
-                         "wall time per search against the sum of its kernels' CUDA-event times (what the per-level "
-                         "host round trips cost), per kernel; one JSON document")
+                         "wall time per search against the sum of its kernels' CUDA-event times, per kernel; "
+                         "one JSON document")
     return ap.parse_args()
 
 
@@ -173,7 +196,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"],
+                 "-lms", "100"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL,
             )
         except OSError:
@@ -210,14 +233,6 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_graph(scale: int):
-    import grafeo_cuda as G
-
-    t = time.time()
-    csr = G.generate_rmat(scale, EDGE_FACTOR, *RMAT_ABC, seed=SEED)
-    return csr, time.time() - t
-
-
 def pinned_copy(arr: np.ndarray):
     """Copies a u32 array into page-locked host memory (torch pin_memory)."""
     import torch
@@ -228,16 +243,83 @@ def pinned_copy(arr: np.ndarray):
     return t, view
 
 
-def bfs_sources(csr, count: int, seed: int) -> np.ndarray:
-    deg = np.diff(csr.offsets)
+def bfs_sources(offsets: np.ndarray, count: int, seed: int) -> np.ndarray:
+    deg = np.diff(offsets)
     rng = np.random.default_rng(seed)
     return rng.choice(np.flatnonzero(deg > 0), size=count, replace=False)
 
 
-def component_edges(csr, dist: np.ndarray) -> int:
+def component_edges(offsets: np.ndarray, dist: np.ndarray) -> int:
     """Undirected edges with both ends in the reached component (Graph500 m)."""
-    deg = np.diff(csr.offsets).astype(np.int64)
+    deg = np.diff(offsets).astype(np.int64)
     return int(deg[dist >= 0].sum() // 2)
+
+
+def directed_dangling_copy(offsets: np.ndarray, targets: np.ndarray, fraction: float, seed: int):
+    """The directed copy of a symmetric CSR in which a seeded uniform
+    `fraction` of the vertices lose their out-edges (they become dangling)."""
+    V = len(offsets) - 1
+    rng = np.random.default_rng(seed)
+    drop = np.zeros(V, dtype=bool)
+    drop[rng.choice(V, size=int(round(fraction * V)), replace=False)] = True
+    deg = np.diff(offsets).astype(np.int64)
+    kept = np.where(drop, 0, deg)
+    new_offsets = np.zeros(V + 1, dtype=np.int64)
+    np.cumsum(kept, out=new_offsets[1:])
+    new_targets = targets[np.repeat(~drop, deg)]
+    return new_offsets.astype(np.uint32), new_targets, int(drop.sum())
+
+
+def workload_config(scale: int, V: int, E_pull: int, n_dangling: int, world: int) -> dict:
+    """The headline's `config`, identical in both arms."""
+    return {
+        "workload": f"R-MAT scale {scale}, edge factor {EDGE_FACTOR}, a=0.57 b=0.19 c=0.19, seed {SEED}, "
+                    f"symmetrised and deduplicated; directed copy with {DANGLING:.0%} of the vertices dangling "
+                    f"(seeded); PageRank damping {DAMPING} until the L1 change is below {TOLERANCE:g} "
+                    f"(at most {MAX_ITERATIONS} iterations); throughput per iteration",
+        "vertices": V,
+        "csr_entries": E_pull,
+        "dangling_vertices": n_dangling,
+        "bytes_per_iteration": pr_bytes(V, E_pull),
+        "l2": "inputs larger than L2 (in-CSR %.2f GB > 126 MB)" % ((4 * (V + 1) + 4 * E_pull) / 1e9),
+        "parallelism": f"replicas x{world}",
+    }
+
+
+def stats(runs_ms: list[float]) -> dict:
+    return {"median_ms": round(statistics.median(runs_ms), 4), "best_ms": round(min(runs_ms), 4),
+            "runs_ms": [round(x, 4) for x in runs_ms]}
+
+
+def platform_info(gpu: str) -> str:
+    """The reference's platform string (harness.rs:162-170)."""
+    return f"{platform.system().lower()} / {platform.machine()} / {socket.gethostname()} / GPU: {gpu}"
+
+
+def harness_record(dataset: str, algorithm: str, V: int, E: int, transfer_s: float, runs_ms: list[float],
+                   teps_edges: float, gpu: str, extra: dict) -> dict:
+    """One GpuBenchmarkResult (harness.rs:14-52): best kernel time over the
+    runs, transfer = CSR upload with validation, teps = edges / best."""
+    best = min(runs_ms) / 1e3
+    return {
+        "dataset": dataset, "algorithm": algorithm, "vertices": V, "edges": E,
+        "time_s": transfer_s + best, "transfer_time_s": transfer_s, "kernel_time_s": best,
+        "teps": teps_edges / best if best > 0 else 0.0,
+        "runs": [x / 1e3 for x in runs_ms],
+        "platform": platform_info(gpu), "gpu_device": gpu,
+        "extra": dict(extra, median_kernel_time_s=statistics.median(runs_ms) / 1e3),
+    }
+
+
+def timed(dev, fn, runs: int = RUNS) -> tuple[list[float], object]:
+    """Device time of `runs` calls (CUDA events around each), after one warm-up call."""
+    out = fn()
+    times = []
+    for _ in range(runs):
+        dev.timer_start()
+        out = fn()
+        times.append(dev.timer_stop())
+    return times, out
 
 
 # ---------------------------------------------------------------- our implementation
@@ -247,19 +329,30 @@ def run_ours(args, d: Dist) -> dict | None:
     import grafeo_cuda as G
 
     dev = G.GpuDevice(d.local_rank)
-    csr, gen_s = make_graph(args.scale)
-    V, E = csr.num_nodes, csr.num_edges
+    t0 = time.perf_counter()
+    g = G.GpuGraph.generate_rmat(dev, args.scale, EDGE_FACTOR, *RMAT_ABC, seed=SEED)
+    sym = g.to_csr()
+    doff, dtgt, ndrop = directed_dangling_copy(sym.offsets, sym.targets, DANGLING, SEED)
+    prep_s = time.perf_counter() - t0
+    V, E = len(doff) - 1, len(dtgt)
     B = pr_bytes(V, E)
-    g = G.GpuGraph.from_csr_arrays(csr, dev)
+    t0 = time.perf_counter()
+    gd = G.GpuGraph.from_csr(doff, dtgt, dev)
+    dev.synchronize()
+    transfer_s = time.perf_counter() - t0
+    gd.pagerank_directed(DAMPING, 2, 0.0, copy_result=False)  # builds the transpose plan
+
+    iters = []
 
     def pr_step():
-        r = g.pagerank_array(DAMPING, PR_ITERATIONS, 0.0, copy_result=False)
-        assert r["iterations"] == PR_ITERATIONS
+        r = gd.pagerank_directed(DAMPING, MAX_ITERATIONS, TOLERANCE, copy_result=False)
+        iters.append(r["iterations"])
 
     # -- value: CSR resident in HBM, device time over K steps, max over ranks
     for _ in range(args.warmup):
         pr_step()
     dev.synchronize()
+    iters.clear()
     d.barrier()
     clocks = ClockSampler(d.local_rank)
     clocks.start()
@@ -272,23 +365,23 @@ def run_ours(args, d: Dist) -> dict | None:
     clk = clocks.stop()
     d.barrier()
     ms_max = d.max(ms)
-    total_bytes = d.sum(float(B) * PR_ITERATIONS * args.steps)
+    total_bytes = d.sum(float(B) * sum(iters))
     value = total_bytes / (ms_max / 1e3) / 1e9
+    step_iterations = iters[-1]
 
     # -- roofline of the dominant kernel: per-launch device time with events
     dev.set_kernel_timing(True)
     dev.reset_stats()
     pr_step()
-    stats = dev.kernel_stats()
+    kstats = dev.kernel_stats()
     dev.set_kernel_timing(False)
     # The dominant kernel runs once per iteration, so one launch moves B bytes.
-    kernel = max(stats, key=lambda k: stats[k][1])
-    tile_n, tile_ms = stats[kernel]
-    step_ms = sum(v[1] for v in stats.values())
+    kernel = max(kstats, key=lambda k: kstats[k][1])
+    tile_n, tile_ms = kstats[kernel]
+    step_ms = sum(v[1] for v in kstats.values())
     tile_avg_ms = tile_ms / max(tile_n, 1)
     peak, peak_kind = measured_peak()
     achieved = B / (tile_avg_ms / 1e3) / 1e9
-    traffic = profiled_traffic(f"pagerank_{kernel}_rmat22.md")
     roofline = {
         "kernel": kernel,
         "bound": "hbm",
@@ -298,36 +391,43 @@ def run_ours(args, d: Dist) -> dict | None:
         "unit": "GB/s",
         "frac": round(achieved / peak, 4),
         "frac_of_8tbs_spec": round(achieved / 8000.0, 4),
-        "traffic": traffic,
+        "traffic": profiled_traffic(f"pagerank_{kernel}_rmat{args.scale}_directed.md"),
         "algorithmic_bytes_per_launch": B,
         "avg_launch_ms": round(tile_avg_ms, 5),
+        "launches_per_step": tile_n,
         "share_of_step": round(tile_ms / step_ms, 4) if step_ms else None,
     }
 
+    # -- the result, for the error against the FP64 oracle (not timed)
+    result = gd.pagerank_directed(DAMPING, MAX_ITERATIONS, TOLERANCE)
+    assert result["iterations"] == step_iterations
+
     # -- e2e through the public API with host buffers
-    off_t, off_pinned = pinned_copy(csr.offsets)
-    tgt_t, tgt_pinned = pinned_copy(csr.targets)
-    ranks_host = None
-    e2e_steps = max(3, min(args.steps, 10))
+    off_t, off_pinned = pinned_copy(doff)
+    tgt_t, tgt_pinned = pinned_copy(dtgt)
+    e2e_steps = max(3, min(args.steps, 8))
+    e2e_iters = []
 
     def e2e_step():
         gg = G.GpuGraph.from_csr(off_pinned, tgt_pinned, dev)
-        r = gg.pagerank_array(DAMPING, PR_ITERATIONS, 0.0)
+        r = gg.pagerank_directed(DAMPING, MAX_ITERATIONS, TOLERANCE)
         del gg
+        e2e_iters.append(r["iterations"])
         return r["ranks"]
 
     e2e_step()
+    e2e_iters.clear()
     d.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         ranks_host = e2e_step()
     e2e_s = d.max(time.perf_counter() - t0)
-    e2e_value = d.sum(float(B) * PR_ITERATIONS * e2e_steps) / e2e_s / 1e9
-    assert ranks_host is not None and ranks_host.shape == (V,)
+    e2e_value = d.sum(float(B) * sum(e2e_iters)) / e2e_s / 1e9
+    assert ranks_host.shape == (V,)
     del off_t, tgt_t
 
     line = {
-        "metric": "PageRank iteration GB/s (algorithmic bytes 4E+12V+4 per iteration)",
+        "metric": METRIC,
         "value": round(value, 2),
         "unit": "GB/s",
         "n_gpus": d.world,
@@ -339,16 +439,10 @@ def run_ours(args, d: Dist) -> dict | None:
         "vs_baseline": None,
         "dtype": "f32 (f64 residual and dangling mass)",
         "data": "synthetic R-MAT (stands in for Graph500/GraphChallenge inputs)",
-        "config": {
-            "workload": f"R-MAT scale {args.scale}, edge factor {EDGE_FACTOR}, a=0.57 b=0.19 c=0.19, seed {SEED}; "
-                        f"PageRank {PR_ITERATIONS} iterations, damping {DAMPING}, per step",
-            "vertices": V,
-            "csr_entries": E,
-            "bytes_per_iteration": B,
-            "l2": "inputs larger than L2 (CSR %.2f GB > 126 MB)" % ((4 * (V + 1) + 4 * E) / 1e9),
-            "parallelism": f"replicas x{d.world}",
-            "graph_generation_s": round(gen_s, 2),
-        },
+        "config": workload_config(args.scale, V, E, ndrop, d.world),
+        "iterations_per_step": step_iterations,
+        "converged": result["converged"],
+        "graph_preparation_s": round(prep_s, 2),
         "gpu_launches": int(launches),
         "roofline": roofline,
         "e2e": {
@@ -356,211 +450,167 @@ def run_ours(args, d: Dist) -> dict | None:
             "unit": "GB/s",
             "h2d_bytes_per_step": 4 * (V + 1) + 4 * E,
             "d2h_bytes_per_step": 4 * V,
-            "what": "GpuGraph.from_csr(pinned host CSR) + pagerank(ranks to host), wall time",
+            "what": "GpuGraph.from_csr(pinned host CSR) + pagerank_directed(ranks to host), wall time; "
+                    "every step uploads, validates, transposes and plans the graph",
+            "ms_per_step": round(e2e_s / e2e_steps * 1e3, 2),
         },
         "clocks": clk,
-        "kernel_ms_per_step": {k: round(v[1], 4) for k, v in stats.items()},
+        "kernel_ms_per_step": {k: round(v[1], 4) for k, v in kstats.items()},
     }
 
     if d.rank == 0 and d.world == 1:
-        line["cpu_baseline"] = cpu_pagerank_sample(csr, B, seconds=10.0)
+        # The FP64 oracle at the same iteration count, timed: the CPU baseline and the error.
+        from oracle import oracle as O
+
+        to, tt = O.transpose_sorted(doff, dtgt)
+        t0 = time.perf_counter()
+        ref = O.pagerank(to, tt, DAMPING, step_iterations, 0.0, out_degree=np.diff(doff))
+        ref_s = time.perf_counter() - t0
+        err = result["ranks"].astype(np.float64) - ref["ranks"]
+        line["accuracy"] = {
+            "l1_error_vs_fp64_oracle": float(np.abs(err).sum()),
+            "linf_error_vs_fp64_oracle": float(np.abs(err).max()),
+            "oracle": f"FP64 power iteration over the same in-CSR, {step_iterations} iterations",
+            "target_l1": 1e-6,
+        }
+        line["cpu_baseline"] = {
+            "value": round(B * step_iterations / ref_s / 1e9, 3),
+            "unit": "GB/s",
+            "cores": O.num_threads(),
+            "kind": "port",
+            "sample": f"the oracle's FP64 PageRank, {step_iterations} iterations on the same in-CSR "
+                      f"({ref_s:.1f} s; the run the error above is taken from)",
+        }
+        del to, tt
     if not args.no_secondary and d.world == 1:
-        line["algorithms"] = secondary(csr, g, dev, args)
+        harness = []
+        # Headline record: kernel time of separate runs of the same step.
+        pr_runs, _ = timed(dev, lambda: gd.pagerank_directed(DAMPING, MAX_ITERATIONS, TOLERANCE, copy_result=False))
+        harness.append(harness_record(
+            f"rmat{args.scale}_seed{SEED}_directed_dangling3", "gpu_pagerank_directed", V, E, transfer_s, pr_runs,
+            float(E) * step_iterations, dev.name,
+            {"iterations": step_iterations, "converged": result["converged"], "damping": DAMPING,
+             "tolerance": TOLERANCE, "gbs_per_iteration_best": B * step_iterations / (min(pr_runs) / 1e3) / 1e9}))
+        del gd
+        algos = {}
+        algos[f"rmat{args.scale}"] = symmetric_block(g, sym, dev, f"rmat{args.scale}_seed{SEED}", harness,
+                                                     decomposition=True, sweep=False, pagerank=False)
+        del g, sym
+        for name, make in (
+            ("rmat22", lambda: G.GpuGraph.generate_rmat(dev, 22, EDGE_FACTOR, *RMAT_ABC, seed=2)),
+            ("er22", lambda: G.GpuGraph.generate_erdos_renyi(dev, 1 << 22, 16 << 22, seed=3)),
+        ):
+            gg = make()
+            algos[name] = symmetric_block(gg, gg.to_csr(), dev, name + ("_seed2" if name == "rmat22" else "_seed3"),
+                                          harness, decomposition=False, sweep=True, pagerank=True)
+            del gg
+        line["algorithms"] = algos
+        line["harness"] = harness
+        if args.save:
+            os.makedirs(args.save, exist_ok=True)
+            for rec in harness:
+                with open(os.path.join(args.save, f"gpu_{rec['algorithm']}_{rec['dataset']}.json"), "w") as f:
+                    json.dump(rec, f, indent=2)
     return line
 
 
-def cpu_pagerank_sample(csr, B: int, seconds: float) -> dict:
-    """Oracle PageRank on the host cores: batches of iterations until ~`seconds`."""
-    from oracle import oracle as O
-
-    iterations, s = 0, 0.0
-    batch = 2
-    while s < seconds and iterations < 2000:
-        t = time.perf_counter()
-        O.pagerank(csr.offsets, csr.targets, DAMPING, batch, 0.0)
-        s += time.perf_counter() - t
-        iterations += batch
-        batch = min(batch * 2, 64)
-    return {
-        "value": round(B * iterations / s / 1e9, 3),
-        "unit": "GB/s",
-        "cores": O.num_threads(),
-        "kind": "port",
-        "sample": f"{iterations} FP64 PageRank iterations of the oracle on the same graph ({s:.1f} s)",
-    }
-
-
-def secondary(csr, g, dev, args, k_truss: bool = True) -> dict:
-    """BFS, triangle counting and k-truss on the resident graph (device time)."""
-    out = {}
-    V, E = csr.num_nodes, csr.num_edges
-    m = E // 2
-    sources = bfs_sources(csr, BFS_SOURCES, SEED)
-    comp_edges = []
-    for s in sources:
-        r = g.bfs_array(int(s))
-        comp_edges.append(component_edges(csr, r["distances"]))
-    total_m = float(sum(comp_edges))
-    for s in sources[:3]:
-        g.bfs_array(int(s), copy_result=False)
-    dev.timer_start()
-    for s in sources:
-        g.bfs_array(int(s), copy_result=False)
-    bfs_ms = dev.timer_stop()
-    bfs_bytes = sum(8 * c + 8 * V for c in comp_edges)
-    out["bfs"] = {
-        "metric": "BFS GTEPS (Graph500: component edges / time, 64 sources)",
-        "value": round(total_m / (bfs_ms / 1e3) / 1e9, 3),
-        "unit": "GTEPS",
-        "ms_per_source": round(bfs_ms / len(sources), 4),
-        "hbm_frac_of_measured": round(bfs_bytes / (bfs_ms / 1e3) / 1e9 / measured_peak()[0], 4),
-    }
-    g.triangle_count()
-    dev.timer_start()
-    reps = 2
-    for _ in range(reps):
-        tc = g.triangle_count()
-    tc_ms = dev.timer_stop() / reps
-    out["triangle_count"] = {
-        "metric": "triangle counting edges/s (undirected edges / time)",
-        "value": round(m / (tc_ms / 1e3), 1),
-        "unit": "edges/s",
-        "ms": round(tc_ms, 3),
-        "triangles": tc["total_triangles"],
-    }
-    # The same BFS and triangle count with the learned schedule installed
-    # (the shipped network), against the fixed rules measured above.
+def symmetric_block(g, csr, dev, dataset: str, harness: list, decomposition: bool, sweep: bool,
+                    pagerank: bool) -> dict:
+    """BFS, triangles (with the learned schedule against the fixed rules),
+    and PageRank, the k-truss sweep or the truss decomposition, on a
+    resident symmetric graph; device times, RUNS runs each."""
+    import grafeo_cuda as G
     from grafeo_cuda import schedule as sched
 
+    out = {"vertices": csr.num_nodes, "csr_entries": csr.num_edges}
+    V, E = csr.num_nodes, csr.num_edges
+    m = E // 2
+    peak = measured_peak()[0]
+    t0 = time.perf_counter()
+    G.GpuGraph.from_csr_arrays(csr, dev)  # upload + validation time, the harness transfer figure
+    dev.synchronize()
+    transfer_s = time.perf_counter() - t0
+    if pagerank:
+        runs, _ = timed(dev, lambda: g.pagerank_array(DAMPING, PR_ITERATIONS, 0.0, copy_result=False))
+        B = pr_bytes(V, E)
+        out["pagerank"] = {"metric": "PageRank iteration GB/s (4E+12V+4 bytes per iteration), 50 iterations",
+                           "value": round(B * PR_ITERATIONS / (statistics.median(runs) / 1e3) / 1e9, 2),
+                           "unit": "GB/s", "hbm_frac_of_measured": round(
+                               B * PR_ITERATIONS / (statistics.median(runs) / 1e3) / 1e9 / peak, 4),
+                           "ms_per_iteration_median": round(statistics.median(runs) / PR_ITERATIONS, 4),
+                           **stats(runs)}
+        harness.append(harness_record(dataset, "gpu_pagerank", V, E, transfer_s, runs, float(E) * PR_ITERATIONS,
+                                      dev.name, {"iterations": PR_ITERATIONS, "damping": DAMPING}))
+    # BFS from 64 seeded non-isolated sources, RUNS runs each.
+    sources = bfs_sources(csr.offsets, BFS_SOURCES, 2)
+    comp, per_source_best, teps = [], [], []
+    total_median = 0.0
+    for s in sources:
+        r = g.bfs_array(int(s))
+        comp.append(component_edges(csr.offsets, r["distances"]))
+        runs, _ = timed(dev, lambda: g.bfs_array(int(s), copy_result=False))
+        per_source_best.append(min(runs))
+        total_median += statistics.median(runs)
+        teps.append(E / (min(runs) / 1e3))
+    m_cc = float(sum(comp))
+    bfs_bytes = sum(8 * c + 8 * V for c in comp)
+    out["bfs"] = {
+        "metric": "BFS GTEPS (Graph500: component edges over time; 64 sources, median of 5 runs each)",
+        "value": round(m_cc / (total_median / 1e3) / 1e9, 3), "unit": "GTEPS",
+        "ms_per_source_median": round(total_median / len(sources), 4),
+        "hbm_frac_of_measured": round(bfs_bytes / (total_median / 1e3) / 1e9 / peak, 4),
+        "reference_teps_harmonic_mean": round(len(teps) / sum(1.0 / t for t in teps), 1),
+    }
+    harness.append(harness_record(dataset, "gpu_bfs", V, E, transfer_s, per_source_best, float(E), dev.name,
+                                  {"sources": len(sources), "runs_are": "best of 5 per source",
+                                   "teps_harmonic_mean": out["bfs"]["reference_teps_harmonic_mean"]}))
+    runs, tc = timed(dev, g.triangle_count)
+    out["triangle_count"] = {"metric": "triangle counting edges/s (undirected edges / time)",
+                             "value": round(m / (statistics.median(runs) / 1e3), 1), "unit": "edges/s",
+                             "triangles": tc["total_triangles"], **stats(runs)}
+    harness.append(harness_record(dataset, "gpu_triangle_count", V, E, transfer_s, runs, float(E), dev.name,
+                                  {"triangles": tc["total_triangles"]}))
+    # The same BFS and triangle count with the learned schedule (the shipped network).
     if os.path.exists(sched.DEFAULT_WEIGHTS):
         ref_dist = g.bfs_array(int(sources[0]))["distances"]
         sched.install(dev)
         try:
             same = bool(np.array_equal(g.bfs_array(int(sources[0]))["distances"], ref_dist))
-            for s in sources[:3]:
-                g.bfs_array(int(s), copy_result=False)
-            dev.timer_start()
+            lmed = 0.0
             for s in sources:
-                g.bfs_array(int(s), copy_result=False)
-            lbfs_ms = dev.timer_stop()
-            tc_l = g.triangle_count()
-            dev.timer_start()
-            for _ in range(reps):
-                tc_l = g.triangle_count()
-            ltc_ms = dev.timer_stop() / reps
+                runs_l, _ = timed(dev, lambda: g.bfs_array(int(s), copy_result=False))
+                lmed += statistics.median(runs_l)
+            runs_t, tc_l = timed(dev, g.triangle_count)
         finally:
             dev.set_schedule(None)
         out["learned_schedule"] = {
-            "bfs_gteps": round(total_m / (lbfs_ms / 1e3) / 1e9, 3),
-            "bfs_speedup_vs_alpha_beta": round(bfs_ms / lbfs_ms, 3),
-            "triangle_count_ms": round(ltc_ms, 3),
-            "triangle_speedup_vs_fixed_buckets": round(tc_ms / ltc_ms, 3),
+            "bfs_gteps": round(m_cc / (lmed / 1e3) / 1e9, 3),
+            "bfs_speedup_vs_alpha_beta": round(total_median / lmed, 3),
+            "triangle_count_ms_median": round(statistics.median(runs_t), 3),
+            "triangle_speedup_vs_fixed_buckets": round(out["triangle_count"]["median_ms"] / statistics.median(runs_t), 3),
             "results_identical": same and tc_l["total_triangles"] == tc["total_triangles"],
         }
-    if not k_truss:
-        return out
-    kt = {}
-    dev.timer_start()
-    for k in range(3, 9):
-        r = g.k_truss_array(k)
-        kt[k] = {"edges": int(len(r["edges"])), "rounds": r["iterations"]}
-    kt_ms = dev.timer_stop()
-    out["k_truss"] = {
-        "metric": "k-truss edges/s (undirected edges / time, k = 3..8 sweep)",
-        "value": round(6 * m / (kt_ms / 1e3), 1),
-        "unit": "edges/s",
-        "ms_total": round(kt_ms, 2),
-        "per_k": kt,
-    }
-    return out
+    if sweep:
+        per_k = {}
 
+        def sweep_once():
+            for k in range(3, 9):
+                r = g.k_truss_array(k)
+                per_k[k] = {"edges": int(len(r["edges"])), "rounds": r["iterations"]}
 
-# ---------------------------------------------------------------- suite (configurations at scale)
-
-
-def pagerank_gbs(g, dev, V: int, E: int, iterations: int = PR_ITERATIONS) -> dict:
-    g.pagerank_array(DAMPING, iterations, 0.0, copy_result=False)
-    dev.timer_start()
-    g.pagerank_array(DAMPING, iterations, 0.0, copy_result=False)
-    ms = dev.timer_stop()
-    return {"metric": "PageRank iteration GB/s (4E+12V+4 bytes per iteration)",
-            "value": round(pr_bytes(V, E) * iterations / (ms / 1e3) / 1e9, 2), "unit": "GB/s",
-            "ms_per_iteration": round(ms / iterations, 4)}
-
-
-def directed_dangling_copy(csr, fraction: float, seed: int):
-    """The directed copy of a symmetric CSR in which a seeded uniform
-    `fraction` of the vertices lose their out-edges (they become dangling)."""
-    V = csr.num_nodes
-    rng = np.random.default_rng(seed)
-    drop = np.zeros(V, dtype=bool)
-    drop[rng.choice(V, size=int(round(fraction * V)), replace=False)] = True
-    deg = np.diff(csr.offsets).astype(np.int64)
-    keep_rows = ~drop
-    offsets = np.zeros(V + 1, dtype=np.int64)
-    np.cumsum(np.where(keep_rows, deg, 0), out=offsets[1:])
-    targets = csr.targets[np.repeat(keep_rows, deg)]
-    return offsets.astype(np.uint32), targets, int(drop.sum())
-
-
-def run_suite(args) -> dict:
-    import grafeo_cuda as G
-    from oracle import oracle as O
-
-    dev = G.GpuDevice(0)
-    out = {"suite": "four algorithms at scale; learned schedule against the fixed rules", "device": dev.name}
-    graphs = (
-        ("rmat22", "R-MAT scale 22, edge factor 16, a=0.57 b=0.19 c=0.19, seed 2",
-         lambda: G.GpuGraph.generate_rmat(dev, 22, EDGE_FACTOR, *RMAT_ABC, seed=2)),
-        ("er22", "Erdos-Renyi G(n = 4,194,304, 16n pairs -> average degree ~32), seed 3",
-         lambda: G.GpuGraph.generate_erdos_renyi(dev, 1 << 22, 16 << 22, seed=3)),
-    )
-    for name, what, make in graphs:
-        g = make()
-        csr = g.to_csr()
-        block = {"graph": what, "vertices": csr.num_nodes, "csr_entries": csr.num_edges,
-                 "pagerank": pagerank_gbs(g, dev, csr.num_nodes, csr.num_edges)}
-        block.update(secondary(csr, g, dev, args))
-        out[name] = block
-        del g
-    # R-MAT 24, seed 5.
-    t0 = time.time()
-    g = G.GpuGraph.generate_rmat(dev, 24, EDGE_FACTOR, *RMAT_ABC, seed=5)
-    dev.synchronize()
-    gen_s = time.time() - t0
-    csr = g.to_csr()
-    V, E = csr.num_nodes, csr.num_edges
-    s24 = {"graph": "R-MAT scale 24, edge factor 16, a=0.57 b=0.19 c=0.19, seed 5", "vertices": V,
-           "csr_entries": E, "device_generation_s": round(gen_s, 3)}
-    # Directed copy with 3 % dangling vertices: PageRank to tol 1e-7 (<= 100 iterations).
-    doff, dtgt, ndrop = directed_dangling_copy(csr, 0.03, seed=5)
-    gd = G.GpuGraph.from_csr(doff, dtgt, dev)
-    gd.pagerank_directed(DAMPING, 2, 0.0)  # builds the transpose plan (not timed)
-    dev.timer_start()
-    pr = gd.pagerank_directed(DAMPING, 100, 1e-7)
-    pr_ms = dev.timer_stop()
-    t0 = time.perf_counter()
-    ref = O.pagerank_directed(doff, dtgt, DAMPING, pr["iterations"], 0.0)
-    ref_s = time.perf_counter() - t0
-    err = np.asarray(pr["ranks"], dtype=np.float64) - ref["ranks"]
-    s24["pagerank_directed"] = {
-        "dangling_vertices": ndrop, "csr_entries": int(len(dtgt)), "damping": DAMPING, "tolerance": 1e-7,
-        "iterations": pr["iterations"], "converged": pr["converged"], "device_ms": round(pr_ms, 2),
-        "ms_per_iteration": round(pr_ms / max(pr["iterations"], 1), 4),
-        "l1_error_vs_fp64_oracle": float(np.abs(err).sum()), "linf_error_vs_fp64_oracle": float(np.abs(err).max()),
-        "oracle": f"FP64 power iteration, same {pr['iterations']} iterations, {O.num_threads()} threads, {ref_s:.1f} s",
-    }
-    del gd
-    # Truss decomposition (every k up to the maximum trussness).
-    dev.timer_start()
-    td = g.truss_decomposition(copy_result=False)
-    td_ms = dev.timer_stop()
-    s24["truss_decomposition"] = {"max_trussness": td["max_trussness"], "rounds": td["rounds"],
-                                  "device_ms": round(td_ms, 1),
-                                  "edges_per_s": round((E // 2) / (td_ms / 1e3), 1)}
-    # BFS and triangles, with the learned schedule against the fixed rules.
-    s24.update(secondary(csr, g, dev, args, k_truss=False))
-    out["rmat24"] = s24
+        runs, _ = timed(dev, sweep_once)
+        out["k_truss"] = {"metric": "k-truss edges/s (undirected edges / time, k = 3..8 sweep)",
+                          "value": round(6 * m / (statistics.median(runs) / 1e3), 1), "unit": "edges/s",
+                          "per_k": per_k, **stats(runs)}
+        harness.append(harness_record(dataset, "gpu_ktruss_sweep_3_8", V, E, transfer_s, runs, 6.0 * E, dev.name,
+                                      {"per_k": per_k}))
+    if decomposition:
+        runs, td = timed(dev, lambda: g.truss_decomposition(copy_result=False), runs=3)
+        out["truss_decomposition"] = {"metric": "truss decomposition edges/s (undirected edges / time)",
+                                      "value": round(m / (statistics.median(runs) / 1e3), 1), "unit": "edges/s",
+                                      "max_trussness": td["max_trussness"], "rounds": td["rounds"], **stats(runs)}
+        harness.append(harness_record(dataset, "gpu_truss_decomposition", V, E, transfer_s, runs, float(E), dev.name,
+                                      {"max_trussness": td["max_trussness"], "rounds": td["rounds"]}))
     return out
 
 
@@ -568,25 +618,34 @@ def run_suite(args) -> dict:
 
 
 def run_reference(args, d: Dist) -> dict | None:
+    """The oracle's FP64 PageRank on the host cores: the graph from the
+    oracle's own generator (equal to the library's, checked by the tests),
+    the same directed copy and in-CSR; each step a bounded sample of
+    iterations of the same workload."""
     if d.rank != 0:
         return None
     from oracle import oracle as O
 
-    csr, gen_s = make_graph(args.scale)
-    V, E = csr.num_nodes, csr.num_edges
+    t0 = time.perf_counter()
+    sym = O.generate_rmat(args.scale, EDGE_FACTOR, *RMAT_ABC, SEED)
+    doff, dtgt, ndrop = directed_dangling_copy(sym.offsets, sym.targets, DANGLING, SEED)
+    del sym
+    to, tt = O.transpose_sorted(doff, dtgt)
+    outdeg = np.diff(doff)
+    prep_s = time.perf_counter() - t0
+    V, E = len(doff) - 1, len(dtgt)
     B = pr_bytes(V, E)
-    sample_iters = PR_ITERATIONS  # the same 50-iteration step as the GPU arm
+    sample_iters = 2  # per step: a bounded sample of the run to tolerance
     for _ in range(max(args.warmup, 1)):
-        O.pagerank(csr.offsets, csr.targets, DAMPING, sample_iters, 0.0)
+        O.pagerank(to, tt, DAMPING, sample_iters, 0.0, out_degree=outdeg)
     t = time.perf_counter()
     for _ in range(args.steps):
-        O.pagerank(csr.offsets, csr.targets, DAMPING, sample_iters, 0.0)
+        O.pagerank(to, tt, DAMPING, sample_iters, 0.0, out_degree=outdeg)
     s = time.perf_counter() - t
     value = B * sample_iters * args.steps / s / 1e9
-    sample = f"{sample_iters} FP64 PageRank iterations per step on the full graph"
     return {
         "impl": "reference",
-        "metric": "PageRank iteration GB/s (algorithmic bytes 4E+12V+4 per iteration)",
+        "metric": METRIC,
         "value": round(value, 3),
         "unit": "GB/s",
         "n_gpus": d.world,
@@ -598,14 +657,11 @@ def run_reference(args, d: Dist) -> dict | None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic R-MAT (stands in for Graph500/GraphChallenge inputs)",
-        "config": {
-            "workload": f"R-MAT scale {args.scale}, edge factor {EDGE_FACTOR}, a=0.57 b=0.19 c=0.19, seed {SEED}; "
-                        f"PageRank damping {DAMPING}",
-            "vertices": V,
-            "csr_entries": E,
-        },
+        "config": workload_config(args.scale, V, E, ndrop, d.world),
+        "graph_preparation_s": round(prep_s, 2),
         "cpu_baseline": {"value": round(value, 3), "unit": "GB/s", "cores": O.num_threads(), "kind": "port",
-                         "sample": sample},
+                         "sample": f"{sample_iters} FP64 PageRank iterations per step on the full in-CSR "
+                                   f"(the GPU step runs the same iterations to tolerance)"},
         "e2e": {"value": round(value, 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "Grafeo 0.6.3's Rust CPU algorithms cannot be built here (no Rust toolchain, crate not vendored); "
                 "the oracle's OpenMP restatement of the same algorithm stands in for them",
@@ -622,6 +678,7 @@ def run_bfs_breakdown() -> dict:
     graphs = (
         ("rmat22", lambda: G.GpuGraph.generate_rmat(dev, 22, EDGE_FACTOR, *RMAT_ABC, seed=2)),
         ("er22", lambda: G.GpuGraph.generate_erdos_renyi(dev, 1 << 22, 16 << 22, seed=3)),
+        ("rmat24", lambda: G.GpuGraph.generate_rmat(dev, 24, EDGE_FACTOR, *RMAT_ABC, seed=5)),
     )
     for name, make in graphs:
         g = make()
@@ -637,16 +694,16 @@ def run_bfs_breakdown() -> dict:
         depth = 0
         for s in sources:
             depth += g.bfs_array(s, copy_result=False)["max_depth"]
-        stats = dev.kernel_stats()
+        kstats = dev.kernel_stats()
         dev.set_kernel_timing(False)
-        kernel_ms = sum(v[1] for v in stats.values())
+        kernel_ms = sum(v[1] for v in kstats.values())
         out[name] = {
             "ms_per_search": round(wall_ms / len(sources), 4),
             "kernel_ms_per_search": round(kernel_ms / len(sources), 4),
             "kernel_share": round(kernel_ms / wall_ms, 3) if wall_ms else None,
             "levels_per_search": depth / len(sources),
             "kernels": {k: {"launches": v[0], "ms": round(v[1], 3)}
-                        for k, v in sorted(stats.items(), key=lambda kv: -kv[1][1])},
+                        for k, v in sorted(kstats.items(), key=lambda kv: -kv[1][1])},
         }
         del g
     return out
@@ -654,9 +711,6 @@ def run_bfs_breakdown() -> dict:
 
 def main():
     args = parse_args()
-    if args.suite:
-        print(json.dumps(run_suite(args)), flush=True)
-        return
     if args.bfs_breakdown:
         print(json.dumps(run_bfs_breakdown()), flush=True)
         return

@@ -557,6 +557,21 @@ Error batch_member(BatchImpl& b, uint32_t index, GraphImpl& g) {
     return dev.sync();
 }
 
+// A captured graph holds the device pointers and the per-batch parameters
+// (S, K, damping, ...) by value: setting new sources or seeds reallocates the
+// buffers it reads, so the capture is dropped, and gcu_batch_replay refuses
+// to run until the caller captures again.
+static void drop_capture(BatchImpl& b) {
+    if (b.exec) {
+        cudaGraphExecDestroy(b.exec);
+        b.exec = nullptr;
+    }
+    if (b.graph) {
+        cudaGraphDestroy(b.graph);
+        b.graph = nullptr;
+    }
+}
+
 Error batch_set_bfs(BatchImpl& b, const uint32_t* sources, uint32_t S, bool keep_distances) {
     DeviceImpl& dev = *b.dev;
     if (S == 0 || S > kMaxBatchSources) return kernel_error("sources per graph must be in 1..=32");
@@ -568,6 +583,8 @@ Error batch_set_bfs(BatchImpl& b, const uint32_t* sources, uint32_t S, bool keep
                                     " of graph " + std::to_string(g) + " out of range (num_nodes = " +
                                     std::to_string(n) + ")");
     }
+    GCU_TRY(dev.sync());  // a replay in flight may still read the old buffers
+    drop_capture(b);
     const uint64_t V = b.u.num_nodes;
     b.S = S;
     b.keep_dist = keep_distances;
@@ -595,6 +612,8 @@ Error batch_set_ppr(BatchImpl& b, const uint32_t* seeds, uint32_t K, float dampi
                                     " of graph " + std::to_string(g) + " out of range (num_nodes = " +
                                     std::to_string(n) + ")");
     }
+    GCU_TRY(dev.sync());  // a replay in flight may still read the old buffers
+    drop_capture(b);
     const uint64_t V = b.u.num_nodes;
     b.K = K;
     b.damping = damping;
@@ -675,14 +694,7 @@ Error batch_capture(BatchImpl& b) {
     GCU_TRY(batch_ensure_tc(b));
     if (!b.bfs_threads) GCU_TRY(autotune(b, launch_bfs, &b.bfs_threads, &b.bfs_tuning));
     if (!b.ppr_threads) GCU_TRY(autotune(b, launch_ppr, &b.ppr_threads, &b.ppr_tuning));
-    if (b.exec) {
-        cudaGraphExecDestroy(b.exec);
-        b.exec = nullptr;
-    }
-    if (b.graph) {
-        cudaGraphDestroy(b.graph);
-        b.graph = nullptr;
-    }
+    drop_capture(b);
     const bool timing = dev.kernel_timing;
     dev.kernel_timing = false;  // no event bookkeeping inside the capture
     GCU_CUDA(cudaStreamBeginCapture(dev.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");

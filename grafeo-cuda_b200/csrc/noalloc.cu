@@ -18,7 +18,11 @@
 //    overlap on the GPU (two host threads, or two streams) race on it;
 //  * the first call on a device looks up the array's device address with that
 //    device current (cudaGetSymbolAddress); make that first call before any
-//    stream capture;
+//    stream capture. The address is kept for the life of the process, which
+//    assumes the device's primary context is never reset (cudaDeviceReset)
+//    between calls;
+//  * each call waits for the caller's stream to finish before it returns (the
+//    count is copied to the host);
 //  * the CSR is not validated here: it must satisfy validate_csr (sorted,
 //    duplicate-free lists, targets < num_nodes), as every GpuGraph does.
 #include <mutex>

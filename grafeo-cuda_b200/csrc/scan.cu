@@ -58,9 +58,11 @@ __global__ void __launch_bounds__(kScanThreads) scan_tile_prefix_kernel(uint32_t
     if (threadIdx.x == 0) *total = carry;
 }
 
-__global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const uint32_t* __restrict__ in, uint64_t n,
+// `in` and `out` may be the same array (callers scan in place), so neither is
+// __restrict__: every thread loads its items into registers before it stores.
+__global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const uint32_t* in, uint64_t n,
                                                                  const uint32_t* __restrict__ tile_prefix,
-                                                                 uint32_t* __restrict__ out) {
+                                                                 uint32_t* out) {
     __shared__ uint32_t warp_tot[32];
     const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
     const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile;
@@ -93,8 +95,8 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const uint32_t
 // One tile (n <= kScanTile): the whole scan in one launch, the total in
 // out[n]. Every thread reads its items before it writes them, so in == out
 // is fine.
-__global__ void __launch_bounds__(kScanThreads) scan_one_tile_kernel(const uint32_t* __restrict__ in, uint32_t n,
-                                                                    uint32_t* __restrict__ out) {
+__global__ void __launch_bounds__(kScanThreads) scan_one_tile_kernel(const uint32_t* in, uint32_t n,
+                                                                    uint32_t* out) {
     __shared__ uint32_t warp_tot[32];
     const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
     uint32_t v[kScanItems];

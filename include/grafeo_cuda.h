@@ -202,7 +202,10 @@ GCU_API gcu_status gcu_triangle_count_oriented(gcu_graph* g, uint64_t* total,
  * cudaMalloc/cudaFree. At most 1,048,576 nodes (else GCU_ERR_KERNEL). All
  * calls on a device share that array: calls that overlap on the GPU race.
  * The first call on a device looks the array up (cudaGetSymbolAddress); make
- * it before any stream capture. */
+ * it before any stream capture. That address is kept for the life of the
+ * process, so the device's primary context must not be reset
+ * (cudaDeviceReset) between calls. Each call waits for `stream` to finish
+ * before it returns. */
 GCU_API gcu_status gcu_triangle_count_oriented_noalloc(const uint32_t* d_offsets, const uint32_t* d_targets,
                                                        uint32_t num_nodes, uint32_t num_edges, void* stream,
                                                        uint64_t* total);
@@ -306,7 +309,9 @@ GCU_API gcu_status gcu_batch_member(gcu_batch* b, uint32_t index, gcu_graph** ou
 /* Triangles of every graph (totals: num_graphs values). */
 GCU_API gcu_status gcu_batch_triangle_count(gcu_batch* b, uint64_t* totals, double* seconds);
 /* Sets the BFS sources: sources[g * S + k] is source k of graph g (local id),
- * 1 <= S <= 32. keep_distances = 0 skips the per-vertex distances. */
+ * 1 <= S <= 32. keep_distances = 0 skips the per-vertex distances. Drops a
+ * captured graph (it reads the buffers this replaces): capture again before
+ * the next gcu_batch_replay. */
 GCU_API gcu_status gcu_batch_set_bfs_sources(gcu_batch* b, const uint32_t* sources, uint32_t S,
                                              int keep_distances);
 /* Runs the BFS; distances (S * num_nodes, source-major: distances[k *
@@ -314,7 +319,8 @@ GCU_API gcu_status gcu_batch_set_bfs_sources(gcu_batch* b, const uint32_t* sourc
  * (num_graphs * S each, graph-major; may be NULL) as gcu_bfs gives them. */
 GCU_API gcu_status gcu_batch_bfs(gcu_batch* b, int32_t* distances, uint32_t* reachable, int32_t* max_depth,
                                  double* seconds);
-/* Sets the personalised PageRank seeds: seeds[g * K + k] (local ids). */
+/* Sets the personalised PageRank seeds: seeds[g * K + k] (local ids). Drops a
+ * captured graph, as gcu_batch_set_bfs_sources does. */
 GCU_API gcu_status gcu_batch_set_pagerank_seeds(gcu_batch* b, const uint32_t* seeds, uint32_t K, float damping,
                                                 uint32_t max_iterations, float tolerance);
 /* Runs it; ranks (num_nodes, may be NULL), iterations and converged

@@ -1,13 +1,14 @@
 // Reference GPU kernels driver — TEST INFRASTRUCTURE ONLY.
 //
 // Compiles grafeo-cuda's own CUDA kernels (crates/grafeo-cuda-algos/kernels/
-// pagerank.cu, bfs.cu, triangle_counting.cu, included from where they lie in
+// pagerank.cu, bfs.cu, triangle_counting.cu, k_truss.cu, included from where they lie in
 // the reference checkout; REF_KERNELS is that directory) for sm_100a and runs
 // them with the launch sequences of the reference's Rust drivers, restated
 // here in C++ (the Rust host code cannot be built in this image):
 //   pagerank    crates/grafeo-cuda-algos/src/pagerank.rs:46-199
 //   bfs         crates/grafeo-cuda-algos/src/bfs.rs:42-131
 //   triangles   crates/grafeo-cuda-algos/src/triangle_counting.rs:40-152
+//   k-truss     crates/grafeo-cuda-algos/src/k_truss.rs:42-161
 // It gives the tests a second oracle (the reference code itself) and the
 // reference kernels' device time on the same B200. Built into oracle/_ref/ by
 // `make -C oracle ref`; nothing in the library links it.
@@ -22,6 +23,11 @@
 #include REF_STR(REF_KERNELS/pagerank.cu)
 #include REF_STR(REF_KERNELS/bfs.cu)
 #include REF_STR(REF_KERNELS/triangle_counting.cu)
+// k_truss.cu's device helper `binary_search` is file-local in the reference's
+// own build (one module per kernel file); its namespace keeps it apart here.
+namespace ref_kt_kernels {
+#include REF_STR(REF_KERNELS/k_truss.cu)
+}  // namespace ref_kt_kernels
 
 namespace {
 
@@ -208,6 +214,58 @@ int ref_triangle_count(const uint32_t* offsets, const uint32_t* targets, uint32_
     cudaFree(fwd_off);
     cudaFree(result);
     return rc;
+}
+
+// k_truss.rs:42-161: per round, support recomputed over the alive entries
+// (thread per node), then every alive entry below k - 2 removed (thread per
+// entry); rounds until one removes nothing; edges u < v that survive, in CSR
+// order. k < 3 returns 3 (the reference's Kernel error); out holds 2 values
+// per surviving edge (at most nnz / 2 edges).
+int ref_k_truss(const uint32_t* offsets, const uint32_t* targets, uint32_t n, uint32_t nnz, uint32_t k, uint32_t* out,
+                uint64_t* num_out, uint32_t* iterations, double* device_ms) {
+    *num_out = 0;
+    *iterations = 0;
+    *device_ms = 0.0;
+    if (k < 3) return 3;
+    if (nnz == 0) return 0;
+    Csr c;
+    if (upload(offsets, targets, n, nnz, c)) return 1;
+    unsigned *support = nullptr, *removed_count = nullptr;
+    unsigned char* removed = nullptr;
+    cudaMalloc(&support, 4ull * nnz);
+    cudaMalloc(&removed, nnz);
+    cudaMalloc(&removed_count, 4);
+    cudaMemset(removed, 0, nnz);
+    const unsigned threshold = k - 2;
+    Timer t;
+    for (;;) {
+        cudaMemset(support, 0, 4ull * nnz);
+        ref_kt_kernels::edge_triangle_support_kernel<<<grid_for(n), kThreads>>>(c.offsets, c.targets, removed, n, support);
+        cudaMemset(removed_count, 0, 4);
+        ref_kt_kernels::edge_filter_kernel<<<grid_for(nnz), kThreads>>>(support, removed, nnz, threshold, removed_count);
+        cudaDeviceSynchronize();
+        *iterations += 1;
+        unsigned h = 0;
+        cudaMemcpy(&h, removed_count, 4, cudaMemcpyDeviceToHost);
+        if (h == 0) break;
+    }
+    *device_ms = t.stop();
+    std::vector<unsigned char> mask(nnz);
+    cudaMemcpy(mask.data(), removed, nnz, cudaMemcpyDeviceToHost);
+    const int err = cudaGetLastError() != cudaSuccess;
+    uint64_t m = 0;
+    for (uint32_t u = 0; u < n; ++u)
+        for (uint32_t idx = offsets[u]; idx < offsets[u + 1]; ++idx)
+            if (targets[idx] > u && !mask[idx]) {
+                out[2 * m] = u;
+                out[2 * m + 1] = targets[idx];
+                ++m;
+            }
+    *num_out = m;
+    cudaFree(support);
+    cudaFree(removed);
+    cudaFree(removed_count);
+    return err;
 }
 
 }  // extern "C"

@@ -34,7 +34,9 @@ def lib() -> C.CDLL:
                                  C.POINTER(C.c_int32), C.POINTER(C.c_double)]
         _lib.ref_triangle_count.argtypes = [u32p, u32p, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64),
                                             C.POINTER(C.c_double)]
-        for f in (_lib.ref_pagerank, _lib.ref_bfs, _lib.ref_triangle_count):
+        _lib.ref_k_truss.argtypes = [u32p, u32p, C.c_uint32, C.c_uint32, C.c_uint32, u32p, C.POINTER(C.c_uint64),
+                                     u32p, C.POINTER(C.c_double)]
+        for f in (_lib.ref_pagerank, _lib.ref_bfs, _lib.ref_triangle_count, _lib.ref_k_truss):
             f.restype = C.c_int
     return _lib
 
@@ -80,3 +82,18 @@ def triangle_count(offsets, targets) -> dict:
         return None
     assert rc == 0, rc
     return {"total_triangles": int(total.value), "device_ms": ms.value}
+
+
+def k_truss(offsets, targets, k: int) -> dict:
+    """{'edges' (m x 2, u < v, CSR order), 'iterations', 'device_ms'}; k < 3
+    raises ValueError (the reference's Kernel error)."""
+    o, t, n, m = _csr(offsets, targets)
+    out = np.zeros(max(m, 2), dtype=np.uint32)
+    count, it, ms = C.c_uint64(), C.c_uint32(), C.c_double()
+    rc = lib().ref_k_truss(o.ctypes.data_as(u32p), t.ctypes.data_as(u32p), n, m, int(k), out.ctypes.data_as(u32p),
+                           C.byref(count), C.byref(it), C.byref(ms))
+    if rc == 3:
+        raise ValueError("k must be >= 3 for k-truss decomposition")
+    assert rc == 0, rc
+    e = int(count.value)
+    return {"edges": out[: 2 * e].reshape(e, 2), "iterations": int(it.value), "device_ms": ms.value}

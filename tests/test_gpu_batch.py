@@ -105,3 +105,43 @@ def test_batch_errors(device):
     b.set_bfs_sources([[0], [0]])
     r = b.bfs()
     assert r["reachable"].tolist() == [[2], [1]] and r["max_depth"].tolist() == [[1], [0]]
+
+
+def test_new_sources_drop_the_capture(device):
+    """A capture reads the source, seed and result buffers by address:
+    setting new sources or seeds drops it, replay refuses until the next
+    capture, and the recaptured replay gives oracle-correct results for the
+    new sources (here with a different S, so the buffers change size)."""
+    b = G.GpuBatch.generate(device, 6, seed=9)
+    csr = b.to_csr()
+    vb = b.vertex_base
+    csrs = []
+    for g in range(b.num_graphs):
+        csrs.append((csr.offsets[vb[g]:vb[g + 1] + 1] - csr.offsets[vb[g]],
+                     csr.targets[csr.offsets[vb[g]]:csr.offsets[vb[g + 1]]] - vb[g]))
+    rng = np.random.default_rng(3)
+    n = [vb[g + 1] - vb[g] for g in range(b.num_graphs)]
+    b.set_bfs_sources(np.array([rng.integers(0, x, 4) for x in n], dtype=np.uint32))
+    b.set_pagerank_seeds(np.array([rng.integers(0, x, 2) for x in n], dtype=np.uint32))
+    b.capture()
+    b.replay()
+    b.results()
+    src = np.array([rng.integers(0, x, 9) for x in n], dtype=np.uint32)
+    b.set_bfs_sources(src)
+    with pytest.raises(GrafeoCudaError) as e:
+        b.replay()
+    assert "no captured graph" in str(e.value)
+    seeds = np.array([rng.integers(0, x, 5) for x in n], dtype=np.uint32)
+    b.capture()
+    b.set_pagerank_seeds(seeds)
+    with pytest.raises(GrafeoCudaError):
+        b.replay()
+    b.capture()
+    b.replay()
+    r = b.results()
+    for g, (o, t) in enumerate(csrs):
+        for k in range(9):
+            ref = O.bfs(o, t, int(src[g, k]))
+            assert np.array_equal(r["distances"][k, vb[g]:vb[g + 1]], ref["distances"]), (g, k)
+        ref = O.pagerank(o, t, 0.85, int(r["iterations"][g]), 0.0, tele=O.seed_vector(len(o) - 1, seeds[g]))
+        assert np.abs(r["ranks"][vb[g]:vb[g + 1]].astype(np.float64) - ref["ranks"]).sum() <= PPR_L1

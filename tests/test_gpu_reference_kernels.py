@@ -4,10 +4,13 @@ oracle/ref_gpu.cu), as a second oracle and as the speed to beat on this GPU.
 * Parity: triangle counts and BFS distances equal the reference kernels' on
   the catalog, messy and random graphs and R-MAT 12/14; PageRank ranks after
   the same number of iterations agree within 1e-5 L1 (both are FP32; the
-  reference sums with float atomics, so its own last bits vary run to run).
+  reference sums with float atomics, so its own last bits vary run to run);
+  k-truss edge sets and round counts for k = 3..8 equal the reference
+  kernels' (crates/grafeo-cuda-algos/kernels/k_truss.cu driven as in
+  src/k_truss.rs:42-161) on the same graphs, self-loop cases included.
 * Speed: PageRank, BFS and triangle counting at R-MAT scale 18 and PageRank and
-  BFS at scale 22, device time of the reference's launch sequence against ours
-  (printed; ours must not be slower).
+  BFS at scale 22, and the k-truss sweep at R-MAT 16, device time of the
+  reference's launch sequence against ours (printed; ours must not be slower).
 """
 from __future__ import annotations
 
@@ -46,6 +49,22 @@ def test_results_equal_the_reference_kernels(device, golden_graphs):
         assert np.abs(mine["ranks"].astype(np.float64) - r["ranks"]).sum() <= 1e-5, name
 
 
+def test_k_truss_equals_the_reference_kernels(device, golden_graphs):
+    cases = small_graphs(golden_graphs)
+    # Self-loops: the reference's first round counts them as common neighbours.
+    sl = G.from_edge_pairs([(0, 1), (1, 2), (0, 2), (2, 3), (3, 3), (2, 2), (1, 1)], 4, True)
+    cases.append(("self-loops", sl.offsets, sl.targets))
+    for name, o, t in cases:
+        g = G.GpuGraph.from_csr(o, t, device)
+        for k in range(3, 9):
+            r = R.k_truss(o, t, k)
+            mine = g.k_truss_array(k)
+            assert np.array_equal(mine["edges"], r["edges"]), (name, k)
+            assert mine["iterations"] == r["iterations"], (name, k)
+    with pytest.raises(ValueError):
+        R.k_truss(cases[0][1], cases[0][2], 2)
+
+
 def _device_ms(device, fn):
     device.synchronize()
     device.timer_start()
@@ -74,3 +93,19 @@ def test_faster_than_the_reference_kernels(device, scale):
     for k, (r_ms, m_ms) in rows.items():
         print(f"R-MAT {scale} {k}: reference kernels {r_ms:.3f} ms, ours {m_ms:.3f} ms, {r_ms / m_ms:.1f}x")
         assert m_ms <= r_ms, k
+
+
+def test_k_truss_faster_than_the_reference_kernels(device):
+    csr = G.generate_rmat(16, 16, seed=2)
+    o, t = csr.offsets, csr.targets
+    ref_ms, mine_ms = 0.0, 0.0
+    for k in range(3, 9):
+        g = G.GpuGraph.from_csr_arrays(csr, device)  # a fresh graph: no cached support
+        ref = R.k_truss(o, t, k)
+        ms = _device_ms(device, lambda: g.k_truss_array(k))
+        assert ms > 0
+        ref_ms += ref["device_ms"]
+        mine_ms += ms
+    print(f"R-MAT 16 k-truss k = 3..8: reference kernels {ref_ms:.1f} ms, ours {mine_ms:.1f} ms, "
+          f"{ref_ms / mine_ms:.1f}x")
+    assert mine_ms <= ref_ms
