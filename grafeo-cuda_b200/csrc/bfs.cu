@@ -308,9 +308,21 @@ __global__ void __launch_bounds__(kTdThreads) bfs_topdown_warp_kernel(
 // last step produced (its counters, plus the host's totals before that step),
 // written to features_out when given; with a network, the chosen variant goes
 // to ctr->choice for the host to read with the counters.
+// Beamer's direction rule (alpha = 14, beta = 24) over the balanced push and
+// the pull, from the state after a step: the fixed schedule, the fallback of
+// the learned one, and the variant the learned pick has to beat by a margin.
+__host__ __device__ __forceinline__ int bfs_fixed_variant(bool symmetric, bool bottom_up, uint64_t frontier_n,
+                                                          uint64_t frontier_m, uint64_t unexplored, uint32_t V) {
+    const double alpha = 14.0, beta = 24.0;
+    if (!symmetric) return kPushBalanced;
+    if (!bottom_up && static_cast<double>(frontier_m) > static_cast<double>(unexplored) / alpha) return kPull;
+    if (bottom_up && static_cast<double>(frontier_n) < static_cast<double>(V) / beta) return kPushBalanced;
+    return bottom_up ? kPull : kPushBalanced;
+}
+
 __global__ void bfs_decide_kernel(const __nv_bfloat16* __restrict__ w, BfsCounters* __restrict__ ctr,
                                   DegreeStats stats, unsigned long long prior_unexplored, uint32_t prior_reached,
-                                  int32_t frontier_level, int frontier_bitmap, unsigned valid_mask,
+                                  int32_t frontier_level, int frontier_bitmap, unsigned valid_mask, uint32_t num_nodes,
                                   float* __restrict__ features_out) {
     const BfsCounters c = *ctr;
     float f[kSchedIn];
@@ -322,7 +334,9 @@ __global__ void bfs_decide_kernel(const __nv_bfloat16* __restrict__ w, BfsCounte
     if (w) {
         float out[kSchedOut];
         sched_forward_warp(w, f, out);
-        if (lane_id() == 0) ctr->choice = sched_pick(out, valid_mask);
+        const int fixed = bfs_fixed_variant((valid_mask >> kPull) & 1u, frontier_bitmap != 0, c.discovered, c.edges,
+                                            prior_unexplored - c.edges, num_nodes);
+        if (lane_id() == 0) ctr->choice = sched_pick_over(out, valid_mask, fixed);
     }
 }
 
@@ -366,14 +380,8 @@ struct BfsState {
     bool bitmap_valid = false;  // bitmap[cur] holds the frontier
 };
 
-// Beamer's direction rule (alpha = 14, beta = 24) over the balanced push and
-// the pull: the fixed schedule, and the fallback of the learned one.
 int fixed_rule(const BfsState& st, bool symmetric, uint32_t V) {
-    constexpr double alpha = 14.0, beta = 24.0;
-    if (!symmetric) return kPushBalanced;
-    if (!st.bottom_up && static_cast<double>(st.frontier_m) > static_cast<double>(st.unexplored) / alpha) return kPull;
-    if (st.bottom_up && static_cast<double>(st.frontier_n) < static_cast<double>(V) / beta) return kPushBalanced;
-    return st.bottom_up ? kPull : kPushBalanced;
+    return bfs_fixed_variant(symmetric, st.bottom_up, st.frontier_n, st.frontier_m, st.unexplored, V);
 }
 
 unsigned valid_variants(bool symmetric) {
@@ -476,7 +484,7 @@ Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reac
     GCU_TRY(start_run(g, w, source));
     if (net)
         GCU_LAUNCH(dev, "bfs_decide", bfs_decide_kernel, 1, 32, 0, net, w.counters.ptr, stats,
-                   static_cast<unsigned long long>(g.num_edges), 0u, 0, 0, valid, nullptr);
+                   static_cast<unsigned long long>(g.num_edges), 0u, 0, 0, valid, g.num_nodes, nullptr);
     GCU_TRY(read_counters(dev, w));
     BfsState st;
     advance(st, *w.host_counters, true, 0, g.num_edges);
@@ -490,7 +498,7 @@ Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reac
         if (net)
             GCU_LAUNCH(dev, "bfs_decide", bfs_decide_kernel, 1, 32, 0, net, w.counters.ptr, stats,
                        static_cast<unsigned long long>(st.unexplored), st.reached, st.level + 1,
-                       variant == kPull ? 1 : 0, valid, nullptr);
+                       variant == kPull ? 1 : 0, valid, g.num_nodes, nullptr);
         GCU_TRY(read_counters(dev, w));
         if (w.host_counters->discovered == 0) break;
         advance(st, *w.host_counters, false, variant, g.num_edges);
@@ -541,7 +549,7 @@ Error bfs_trace(GraphImpl& g, uint32_t source, uint64_t explore_seed, std::vecto
     GCU_TRY(feats.allocate(dev, kSchedIn));
     GCU_TRY(start_run(g, w, source));
     GCU_LAUNCH(dev, "bfs_decide", bfs_decide_kernel, 1, 32, 0, nullptr, w.counters.ptr, stats,
-               static_cast<unsigned long long>(g.num_edges), 0u, 0, 0, valid, feats.ptr);
+               static_cast<unsigned long long>(g.num_edges), 0u, 0, 0, valid, g.num_nodes, feats.ptr);
     GCU_TRY(read_counters(dev, w));
     BfsState st;
     advance(st, *w.host_counters, true, 0, g.num_edges);
@@ -587,7 +595,7 @@ Error bfs_trace(GraphImpl& g, uint32_t source, uint64_t explore_seed, std::vecto
         GCU_TRY(launch_step(g, w, take, st));
         GCU_LAUNCH(dev, "bfs_decide", bfs_decide_kernel, 1, 32, 0, nullptr, w.counters.ptr, stats,
                    static_cast<unsigned long long>(st.unexplored), st.reached, st.level + 1, take == kPull ? 1 : 0,
-                   valid, feats.ptr);
+                   valid, g.num_nodes, feats.ptr);
         BfsCounters vc[kSchedOut];
         GCU_CUDA(cudaMemcpyAsync(vc, variant_ctr.ptr, sizeof(vc), cudaMemcpyDeviceToHost, dev.stream), "copy");
         GCU_CUDA(cudaMemcpyAsync(host_feats.data(), feats.ptr, 4 * kSchedIn, cudaMemcpyDeviceToHost, dev.stream),

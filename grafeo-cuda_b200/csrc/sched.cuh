@@ -132,4 +132,18 @@ __host__ __device__ __forceinline__ int sched_pick(const float* out, unsigned va
     return best;
 }
 
+// The network's pick replaces the fixed rule's variant only where it predicts
+// that variant at least 2^kSchedMarginLog2 (1.15x) slower than its pick. On
+// graphs the fixed rule already serves well (R-MAT and Erdos-Renyi levels,
+// where the alpha/beta rule is near the best schedule) the remaining predicted
+// gains are within the network's error, and following them costs time; the
+// large gains (long-diameter graphs, small frontiers) are far above the margin.
+constexpr float kSchedMarginLog2 = 0.2f;
+
+__host__ __device__ __forceinline__ int sched_pick_over(const float* out, unsigned valid_mask, int fixed) {
+    const int best = sched_pick(out, valid_mask);
+    if (best < 0 || best == fixed || fixed < 0 || !((valid_mask >> fixed) & 1u)) return best;
+    return out[fixed] - out[best] >= kSchedMarginLog2 ? best : fixed;
+}
+
 }  // namespace gcu

@@ -263,7 +263,7 @@ __global__ void tc_decide_kernel(const __nv_bfloat16* __restrict__ w, const uint
         if (w) {
             float out[kSchedOut];
             sched_forward_warp(w, f, out);
-            if (lane_id() == 0) choices[c] = sched_pick(out, bucket_valid(c));
+            if (lane_id() == 0) choices[c] = sched_pick_over(out, bucket_valid(c), bucket_fixed(c));
         }
     }
 }

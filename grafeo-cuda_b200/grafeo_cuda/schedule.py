@@ -41,6 +41,11 @@ HELDOUT_SEED_BASE = 1_000_000  # held-out graph seeds start here; training seeds
 # ---------------------------------------------------------------- corpus
 
 
+# The device's kSchedMarginLog2 (csrc/sched.cuh): the learned pick must be
+# predicted at least 2^MARGIN_LOG2 faster than the fixed rule's variant.
+MARGIN_LOG2 = 0.2
+
+
 def corpus(count: int, seed: int, scale_range=(16, 22)) -> list[dict]:
     """Seeded graph specs, one quarter each R-MAT, grid, geometric and
     Erdos-Renyi (uniform neighbours: no hubs and no locality)."""
@@ -161,13 +166,20 @@ def train(device: G.GpuDevice, data: dict, steps: int = 6000, batch: int = 1024,
 
 
 def choose(device: G.GpuDevice, weights, data: dict) -> np.ndarray:
-    """The network's pick for every decision (the fixed rule where it abstains)."""
+    """The network's pick for every decision as the device makes it: the
+    fixed rule where the network abstains (a non-finite prediction) or where
+    it predicts its pick less than 2^MARGIN_LOG2 faster than the fixed rule's
+    variant."""
     pred = G.schedule_forward(device, weights, data["features"])
     valid = np.stack([(data["valid"] >> c) & 1 for c in range(G.SCHEDULE_OUTPUTS)], axis=1).astype(bool)
     pred = np.where(valid, pred, np.inf)
     pick = np.argmin(pred, axis=1)
-    bad = ~np.isfinite(pred[np.arange(len(pick)), pick]) if len(pick) else np.zeros(0, bool)
-    return np.where(bad, data["fixed_rule"], pick)
+    idx = np.arange(len(pick))
+    fixed = data["fixed_rule"].astype(np.int64)
+    bad = ~np.all(np.isfinite(np.where(valid, pred, 0.0)), axis=1) if len(pick) else np.zeros(0, bool)
+    with np.errstate(invalid="ignore"):
+        keep = (pick == fixed) | (pred[idx, fixed] - pred[idx, pick] >= MARGIN_LOG2)
+    return np.where(bad | ~keep, fixed, pick)
 
 
 def trace_gain(device: G.GpuDevice, weights, data: dict) -> dict:

@@ -189,3 +189,16 @@ def test_wide_frontier_fixture_shape():
     c = G.from_edge_pairs(pairs, n, True)
     r = O.bfs(c.offsets, c.targets, 0)
     assert r["distances"].tolist() == expected.tolist() and r["max_depth"] == 5
+
+
+def test_schedule_margin_matches_the_device_constant():
+    """The Python evaluation of the learned schedule applies the same margin
+    over the fixed rule as the device's decide kernels."""
+    import os
+    import re
+
+    from grafeo_cuda import schedule
+
+    src = open(os.path.join(os.path.dirname(__file__), "..", "grafeo-cuda_b200", "csrc", "sched.cuh")).read()
+    value = float(re.search(r"kSchedMarginLog2\s*=\s*([0-9.]+)f", src).group(1))
+    assert value == schedule.MARGIN_LOG2
