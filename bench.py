@@ -86,9 +86,9 @@ def parse_args():
     ap.add_argument("--no-secondary", action="store_true", help="skip the algorithms block and the harness records")
     ap.add_argument("--save", metavar="DIR", help="also write every harness record to DIR/gpu_<algorithm>_<dataset>.json")
     ap.add_argument("--bfs-breakdown", action="store_true",
-                    help="instead of the headline: BFS from 16 random sources on R-MAT 22 and Erdos-Renyi 2^22, "
-                         "wall time per search against the sum of its kernels' CUDA-event times, per kernel; "
-                         "one JSON document")
+                    help="instead of the headline: BFS from 16 random sources on R-MAT 22, Erdos-Renyi 2^22 and "
+                         "R-MAT 24, device time per search with the level loop on the device and on the host, "
+                         "against the sum of its kernels' CUDA-event times, per kernel; one JSON document")
     return ap.parse_args()
 
 
@@ -669,8 +669,10 @@ def run_reference(args, d: Dist) -> dict | None:
 
 
 def run_bfs_breakdown() -> dict:
-    """Device time of 16 searches (CUDA events around the run) against the sum
-    of their kernels' own event times, and the per-kernel split."""
+    """Device time of 16 searches (CUDA events around the run) with the level
+    loop on the device and driven from the host, against the sum of the
+    kernels' own event times (host-driven, per-kernel timing on), and the
+    per-kernel split."""
     import grafeo_cuda as G
 
     dev = G.GpuDevice(0)
@@ -683,12 +685,17 @@ def run_bfs_breakdown() -> dict:
     for name, make in graphs:
         g = make()
         sources = [int(x) for x in np.random.default_rng(1).integers(0, g.num_nodes, 16)]
-        for s in sources[:3]:
-            g.bfs_array(s, copy_result=False)
-        dev.timer_start()
-        for s in sources:
-            g.bfs_array(s, copy_result=False)
-        wall_ms = dev.timer_stop()
+        loop_ms = {}
+        for on in (True, False):
+            dev.set_bfs_device_loop(on)
+            for s in sources[:3]:
+                g.bfs_array(s, copy_result=False)
+            dev.timer_start()
+            for s in sources:
+                g.bfs_array(s, copy_result=False)
+            loop_ms[on] = dev.timer_stop()
+        dev.set_bfs_device_loop(True)
+        wall_ms = loop_ms[False]
         dev.set_kernel_timing(True)
         dev.reset_stats()
         depth = 0
@@ -698,6 +705,7 @@ def run_bfs_breakdown() -> dict:
         dev.set_kernel_timing(False)
         kernel_ms = sum(v[1] for v in kstats.values())
         out[name] = {
+            "ms_per_search_device_loop": round(loop_ms[True] / len(sources), 4),
             "ms_per_search": round(wall_ms / len(sources), 4),
             "kernel_ms_per_search": round(kernel_ms / len(sources), 4),
             "kernel_share": round(kernel_ms / wall_ms, 3) if wall_ms else None,

@@ -58,6 +58,22 @@ enum BfsVariant : int {
     kPull = 2,          // bottom-up over the frontier bitmap (symmetric graphs only)
 };
 
+// Where a device-driven run stands between two steps (the device twin of the
+// host loop's BfsState, kept in device memory and read by every step kernel).
+struct BfsDevState {
+    unsigned long long frontier_m;  // out-edges of the frontier
+    unsigned long long unexplored;  // out-edges of vertices not labelled yet
+    uint32_t frontier_n;            // vertices labelled by the last step
+    uint32_t frontier_q;            // of those, queued (out-degree > 0)
+    uint32_t reached;
+    int32_t level;                  // level of the frontier
+    uint32_t cur;                   // queue[cur] / bitmap[cur] hold the frontier
+    uint32_t bitmap_valid;          // the last step was a pull: bitmap[cur] holds the frontier
+    int32_t variant;                // the step the SWITCH node runs next (kSchedOut: none)
+    uint32_t first;                 // the counters are the source's, not a step's
+    uint32_t failed;                // the loop stopped on a state no search can reach
+};
+
 struct BfsWork {
     DeviceBuffer<int32_t> dist;
     DeviceBuffer<uint32_t> visited;
@@ -67,10 +83,21 @@ struct BfsWork {
     DeviceBuffer<BfsCounters> counters;
     BfsCounters* host_counters = nullptr;  // pinned
     int symmetric = -1;                    // -1 unknown, 0 no, 1 yes
+    // device-driven level loop (built on first use, per schedule network)
+    DeviceBuffer<BfsDevState> loop_state;
+    DeviceBuffer<uint32_t> loop_scan_sums;
+    BfsDevState* host_loop_state = nullptr;  // pinned
+    cudaGraph_t loop_graph = nullptr;
+    cudaGraphExec_t loop_exec = nullptr;
+    const void* loop_net = nullptr;  // the schedule network the graph reads (NULL: fixed rule)
+    bool loop_unavailable = false;   // the driver refused the graph: the host drives the levels
 };
 
 void destroy_bfs_work(BfsWork* w) {
     if (!w) return;
+    if (w->loop_exec) cudaGraphExecDestroy(w->loop_exec);
+    if (w->loop_graph) cudaGraphDestroy(w->loop_graph);
+    if (w->host_loop_state) cudaFreeHost(w->host_loop_state);
     if (w->host_counters) cudaFreeHost(w->host_counters);
     delete w;
 }
@@ -145,17 +172,17 @@ __global__ void bfs_queue_degrees_kernel(const uint32_t* __restrict__ offsets, c
     }
 }
 
-// Top-down: block b expands frontier edges [b*kTdTile, (b+1)*kTdTile).
-__global__ void __launch_bounds__(kTdThreads) bfs_topdown_kernel(
-    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, const uint32_t* __restrict__ queue,
-    uint32_t qsize, const uint32_t* __restrict__ qscan, int32_t* __restrict__ dist, uint32_t* __restrict__ visited,
-    uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr, int32_t next_level) {
+// Top-down: the block expands frontier edges [e0, e0 + kTdTile) of `total`
+// (every thread of the block calls it with the same tile).
+__device__ __forceinline__ void topdown_tile(const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
+                                             const uint32_t* __restrict__ queue, uint32_t qsize,
+                                             const uint32_t* __restrict__ qscan, uint32_t total, uint64_t e0,
+                                             int32_t* __restrict__ dist, uint32_t* __restrict__ visited,
+                                             uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr,
+                                             int32_t next_level, Tally& tally) {
     __shared__ uint32_t s_scan[kTdTile + 1];
     __shared__ uint32_t s_start[kTdTile + 1];
     __shared__ uint32_t s_range[2];
-    const uint32_t total = qscan[qsize];
-    const uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kTdTile;
-    if (e0 >= total) return;
     const uint32_t e1 = static_cast<uint32_t>(min_u64(e0 + kTdTile, total));
     if (threadIdx.x < 2) {
         // Largest frontier index i with qscan[i] <= e (each queued vertex owns >= 1 edge).
@@ -178,7 +205,6 @@ __global__ void __launch_bounds__(kTdThreads) bfs_topdown_kernel(
         s_start[k] = offsets[queue[i0 + k]];
     }
     __syncthreads();
-    Tally tally;
 #pragma unroll
     for (int q = 0; q < kTdItems; ++q) {
         const uint32_t e = static_cast<uint32_t>(e0) + q * kTdThreads + threadIdx.x;
@@ -199,6 +225,18 @@ __global__ void __launch_bounds__(kTdThreads) bfs_topdown_kernel(
         }
         record_discovery(found, v, offsets, dist, next_level, next_queue, ctr, tally);
     }
+}
+
+// Top-down: block b expands frontier edges [b*kTdTile, (b+1)*kTdTile).
+__global__ void __launch_bounds__(kTdThreads) bfs_topdown_kernel(
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, const uint32_t* __restrict__ queue,
+    uint32_t qsize, const uint32_t* __restrict__ qscan, int32_t* __restrict__ dist, uint32_t* __restrict__ visited,
+    uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr, int32_t next_level) {
+    const uint32_t total = qscan[qsize];
+    const uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kTdTile;
+    if (e0 >= total) return;
+    Tally tally;
+    topdown_tile(offsets, targets, queue, qsize, qscan, total, e0, dist, visited, next_queue, ctr, next_level, tally);
     flush_tally(tally, ctr);
 }
 
@@ -224,7 +262,7 @@ __device__ __forceinline__ bool in_frontier(const uint32_t* __restrict__ frontie
 // 32 consecutive entries per step (coalesced) with a ballot to stop at the
 // first parent, so a long list neither serialises one lane nor stalls the
 // other 31.
-__global__ void __launch_bounds__(kBuThreads) bfs_bottomup_kernel(
+__device__ __forceinline__ void bottomup_body(
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t V,
     const uint32_t* __restrict__ frontier, uint32_t* __restrict__ next_frontier, uint32_t* __restrict__ visited,
     int32_t* __restrict__ dist, uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr,
@@ -277,9 +315,17 @@ __global__ void __launch_bounds__(kBuThreads) bfs_bottomup_kernel(
     flush_tally(tally, ctr);
 }
 
+__global__ void __launch_bounds__(kBuThreads) bfs_bottomup_kernel(
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t V,
+    const uint32_t* __restrict__ frontier, uint32_t* __restrict__ next_frontier, uint32_t* __restrict__ visited,
+    int32_t* __restrict__ dist, uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr,
+    int32_t next_level) {
+    bottomup_body(offsets, targets, V, frontier, next_frontier, visited, dist, next_queue, ctr, next_level);
+}
+
 // Top-down, one warp per frontier vertex (no degree scan: one launch, for
 // frontiers whose edges are few or evenly spread).
-__global__ void __launch_bounds__(kTdThreads) bfs_topdown_warp_kernel(
+__device__ __forceinline__ void topdown_warp_body(
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, const uint32_t* __restrict__ queue,
     uint32_t qsize, int32_t* __restrict__ dist, uint32_t* __restrict__ visited, uint32_t* __restrict__ next_queue,
     BfsCounters* __restrict__ ctr, int32_t next_level) {
@@ -302,6 +348,13 @@ __global__ void __launch_bounds__(kTdThreads) bfs_topdown_warp_kernel(
         }
     }
     flush_tally(tally, ctr);
+}
+
+__global__ void __launch_bounds__(kTdThreads) bfs_topdown_warp_kernel(
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, const uint32_t* __restrict__ queue,
+    uint32_t qsize, int32_t* __restrict__ dist, uint32_t* __restrict__ visited, uint32_t* __restrict__ next_queue,
+    BfsCounters* __restrict__ ctr, int32_t next_level) {
+    topdown_warp_body(offsets, targets, queue, qsize, dist, visited, next_queue, ctr, next_level);
 }
 
 // One warp: the features of the decision before expanding the frontier the
@@ -338,6 +391,174 @@ __global__ void bfs_decide_kernel(const __nv_bfloat16* __restrict__ w, BfsCounte
                                             prior_unexplored - c.edges, num_nodes);
         if (lane_id() == 0) ctr->choice = sched_pick_over(out, valid_mask, fixed);
     }
+}
+
+// ---------------------------------------------------------------- device-driven level loop
+//
+// The host-driven loop reads the level counters back after every step (one
+// copy and one synchronisation per level). The device-driven loop runs a
+// whole search as one CUDA graph: a WHILE node whose body is a one-warp
+// decide kernel followed by a SWITCH node over the three step variants. The
+// decide kernel folds the last step's counters into BfsDevState exactly as
+// the host's `advance` does, ends the loop where the host loop stops (empty
+// frontier, or a step that labelled nothing), picks the next variant (the
+// alpha/beta rule, or the learned schedule with its margin), and sets the
+// SWITCH value; each step kernel reads its frontier size, level and queue
+// parity from the state. The grids are fixed when the graph is captured and
+// the kernels stride over what the state holds.
+
+__global__ void bfs_loop_init_kernel(const uint32_t* __restrict__ offsets, uint32_t source,
+                                     int32_t* __restrict__ dist, uint32_t* __restrict__ visited,
+                                     uint32_t* __restrict__ queue0, BfsCounters* __restrict__ ctr,
+                                     BfsDevState* __restrict__ st) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    dist[source] = 0;
+    visited[source >> 5] |= 1u << (source & 31);
+    const uint32_t deg = offsets[source + 1] - offsets[source];
+    queue0[0] = source;
+    BfsCounters c{};
+    c.discovered = 1;
+    c.queued = deg > 0 ? 1u : 0u;
+    c.edges = deg;
+    *ctr = c;
+    BfsDevState s{};
+    s.first = 1;
+    s.variant = kSchedOut;
+    *st = s;
+}
+
+__global__ void bfs_loop_decide_kernel(const __nv_bfloat16* __restrict__ w, BfsCounters* __restrict__ ctr,
+                                       BfsDevState* __restrict__ st, DegreeStats stats, unsigned long long num_edges,
+                                       uint32_t V, unsigned valid_mask, cudaGraphConditionalHandle h_loop,
+                                       cudaGraphConditionalHandle h_step) {
+    const BfsCounters c = *ctr;
+    BfsDevState s = *st;
+    bool stop = false;
+    if (s.first) {
+        s.first = 0;
+        s.unexplored = num_edges - c.edges;
+        s.reached = 1;
+        s.level = 0;
+    } else if (c.discovered == 0) {
+        stop = true;  // the step labelled nothing: level and reached stay
+    } else {
+        s.level += 1;
+        s.reached += c.discovered;
+        s.unexplored -= c.edges;
+        s.cur ^= 1u;
+        s.bitmap_valid = s.variant == kPull ? 1u : 0u;
+    }
+    if (!stop) {
+        s.frontier_n = c.discovered;
+        s.frontier_q = c.queued;
+        s.frontier_m = c.edges;
+        stop = s.frontier_q == 0;
+    }
+    // A search labels each vertex once, so it ends within V levels with at
+    // most V vertices reached and at most V queued; state past these bounds
+    // can only come from a fault, and it ends the loop with the error flag
+    // set instead of looping or indexing past the queues.
+    if (!stop && (static_cast<uint64_t>(s.level) >= V || s.reached > V || s.frontier_q > V)) {
+        stop = true;
+        s.failed = 1;
+    }
+    int variant = kSchedOut;
+    if (!stop) {
+        variant = bfs_fixed_variant((valid_mask >> kPull) & 1u, s.bitmap_valid != 0, s.frontier_n, s.frontier_m,
+                                    s.unexplored, V);
+        if (w) {
+            float f[kSchedIn];
+            bfs_features(f, static_cast<float>(s.frontier_n), static_cast<float>(s.frontier_m),
+                         static_cast<float>(s.unexplored), s.level, stats, s.bitmap_valid != 0,
+                         static_cast<float>(s.reached));
+            float out[kSchedOut];
+            sched_forward_warp(w, f, out);
+            const int pick = sched_pick_over(out, valid_mask, variant);
+            if (pick >= 0) variant = pick;
+        }
+    }
+    __syncwarp();
+    if (lane_id() == 0) {
+        s.variant = variant;
+        *st = s;
+        *ctr = BfsCounters{};
+        cudaGraphSetConditional(h_step, static_cast<unsigned>(variant));
+        cudaGraphSetConditional(h_loop, stop ? 0u : 1u);
+    }
+}
+
+__global__ void __launch_bounds__(kTdThreads) bfs_topdown_warp_loop_kernel(
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t* queue0, uint32_t* queue1,
+    int32_t* __restrict__ dist, uint32_t* __restrict__ visited, BfsCounters* __restrict__ ctr,
+    const BfsDevState* __restrict__ st) {
+    const uint32_t cur = st->cur;
+    topdown_warp_body(offsets, targets, cur ? queue1 : queue0, st->frontier_q, dist, visited, cur ? queue0 : queue1,
+                      ctr, st->level + 1);
+}
+
+__global__ void bfs_queue_degrees_loop_kernel(const uint32_t* __restrict__ offsets, const uint32_t* queue0,
+                                              const uint32_t* queue1, const BfsDevState* __restrict__ st,
+                                              uint32_t* __restrict__ deg) {
+    const uint32_t* queue = st->cur ? queue1 : queue0;
+    const uint32_t n = st->frontier_q;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t u = queue[i];
+        deg[i] = offsets[u + 1] - offsets[u];
+    }
+}
+
+// Balanced top-down over the scanned frontier degrees: blocks stride over the
+// kTdTile-edge tiles of the frontier.
+__global__ void __launch_bounds__(kTdThreads) bfs_topdown_loop_kernel(
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t* queue0, uint32_t* queue1,
+    const uint32_t* __restrict__ qscan, int32_t* __restrict__ dist, uint32_t* __restrict__ visited,
+    BfsCounters* __restrict__ ctr, const BfsDevState* __restrict__ st) {
+    const uint32_t cur = st->cur, qsize = st->frontier_q;
+    const int32_t next_level = st->level + 1;
+    const uint32_t total = qscan[qsize];
+    const uint32_t* queue = cur ? queue1 : queue0;
+    uint32_t* next_queue = cur ? queue0 : queue1;
+    Tally tally;
+    const uint64_t tiles = ceil_div_u64(total, kTdTile);
+    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        topdown_tile(offsets, targets, queue, qsize, qscan, total, t * kTdTile, dist, visited, next_queue, ctr,
+                     next_level, tally);
+        __syncthreads();  // the tile's shared arrays are reused by the next tile
+    }
+    flush_tally(tally, ctr);
+}
+
+// Before a pull that follows a push: the frontier bitmap from the queue.
+__global__ void bfs_bitmap_clear_loop_kernel(uint32_t* bitmap0, uint32_t* bitmap1, uint64_t words,
+                                             const BfsDevState* __restrict__ st) {
+    if (st->bitmap_valid) return;
+    uint32_t* bitmap = st->cur ? bitmap1 : bitmap0;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < words;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        bitmap[i] = 0;
+}
+
+__global__ void bfs_queue_to_bitmap_loop_kernel(const uint32_t* queue0, const uint32_t* queue1, uint32_t* bitmap0,
+                                                uint32_t* bitmap1, const BfsDevState* __restrict__ st) {
+    if (st->bitmap_valid) return;
+    const uint32_t* queue = st->cur ? queue1 : queue0;
+    uint32_t* bitmap = st->cur ? bitmap1 : bitmap0;
+    const uint32_t n = st->frontier_q;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t u = queue[i];
+        atomicOr(bitmap + (u >> 5), 1u << (u & 31));
+    }
+}
+
+__global__ void __launch_bounds__(kBuThreads) bfs_bottomup_loop_kernel(
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t V, uint32_t* bitmap0,
+    uint32_t* bitmap1, uint32_t* __restrict__ visited, int32_t* __restrict__ dist, uint32_t* queue0,
+    uint32_t* queue1, BfsCounters* __restrict__ ctr, const BfsDevState* __restrict__ st) {
+    const uint32_t cur = st->cur;
+    bottomup_body(offsets, targets, V, cur ? bitmap1 : bitmap0, cur ? bitmap0 : bitmap1, visited, dist,
+                  cur ? queue0 : queue1, ctr, st->level + 1);
 }
 
 // ---------------------------------------------------------------- host
@@ -463,6 +684,145 @@ void advance(BfsState& st, const BfsCounters& c, bool first, int variant, uint64
     st.frontier_m = c.edges;
 }
 
+// Captures the launches `f` makes on the device stream into `target` (a
+// conditional node's body graph).
+template <class F>
+Error capture_into(DeviceImpl& dev, cudaGraph_t target, F&& f) {
+    GCU_CUDA(cudaStreamBeginCaptureToGraph(dev.stream, target, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+             "cudaStreamBeginCaptureToGraph");
+    const Error e = f();
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(dev.stream, &captured);
+    GCU_TRY(e);
+    if (ce != cudaSuccess) return driver_error(ce, "cudaStreamEndCapture");
+    return ok();
+}
+
+// The graph of a device-driven search: WHILE(loop) { decide; SWITCH(step) {
+// push with a warp per vertex | balanced push | pull } }. Everything it reads
+// lives in the BfsWork buffers and the graph's CSR; the source is labelled by
+// bfs_loop_init_kernel before each launch.
+Error build_loop_graph(GraphImpl& g, BfsWork& w) {
+    DeviceImpl& dev = *g.dev;
+    if (w.loop_exec) {
+        cudaGraphExecDestroy(w.loop_exec);
+        w.loop_exec = nullptr;
+    }
+    if (w.loop_graph) {
+        cudaGraphDestroy(w.loop_graph);
+        w.loop_graph = nullptr;
+    }
+    const uint32_t V = g.num_nodes;
+    const uint64_t words = ceil_div_u64(V, 32);
+    if (!w.loop_state.ptr) {
+        GCU_TRY(w.loop_state.allocate(dev, 1));
+        GCU_TRY(w.loop_scan_sums.allocate(dev, scan_device_n_tiles(V)));
+        GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&w.host_loop_state), sizeof(BfsDevState)), "cudaMallocHost");
+    }
+    const __nv_bfloat16* net = reinterpret_cast<const __nv_bfloat16*>(dev.schedule);
+    DegreeStats stats;
+    if (net) GCU_TRY(degree_stats(g, &stats));
+    const bool sym = w.symmetric == 1;
+    const unsigned valid = valid_variants(sym);
+    BfsDevState* st = w.loop_state.ptr;
+    const uint32_t* n_ptr = &st->frontier_q;
+    const unsigned cap = static_cast<unsigned>(dev.sm_count) * 16;
+    const unsigned vgrid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(V, 256), cap)));
+    const unsigned bu_grid =
+        static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(words * 32, kBuThreads), cap)));
+    const unsigned wgrid =
+        static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(V, kTdThreads / 32), cap)));
+    const unsigned td_grid = static_cast<unsigned>(dev.sm_count) * 8;
+
+    cudaGraph_t graph = nullptr;
+    GCU_CUDA(cudaGraphCreate(&graph, 0), "cudaGraphCreate");
+    struct Owner {
+        cudaGraph_t g;
+        ~Owner() {
+            if (g) cudaGraphDestroy(g);
+        }
+    } owner{graph};
+    cudaGraphConditionalHandle h_loop = 0, h_step = 0;
+    GCU_CUDA(cudaGraphConditionalHandleCreate(&h_loop, graph, 1, cudaGraphCondAssignDefault),
+             "cudaGraphConditionalHandleCreate");
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = h_loop;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t while_node = nullptr;
+    GCU_CUDA(cudaGraphAddNode(&while_node, graph, nullptr, 0, &wp), "cudaGraphAddNode (while)");
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    GCU_CUDA(cudaGraphConditionalHandleCreate(&h_step, body, 0, 0), "cudaGraphConditionalHandleCreate");
+    GCU_TRY(capture_into(dev, body, [&]() -> Error {
+        GCU_LAUNCH(dev, "bfs_loop_decide", bfs_loop_decide_kernel, 1, 32, 0, net, w.counters.ptr, st, stats,
+                   static_cast<unsigned long long>(g.num_edges), V, valid, h_loop, h_step);
+        return ok();
+    }));
+    cudaGraphNode_t decide_node = nullptr;
+    size_t nodes = 1;
+    GCU_CUDA(cudaGraphGetNodes(body, &decide_node, &nodes), "cudaGraphGetNodes");
+    if (nodes != 1) return kernel_error("BFS loop graph: unexpected body");
+    cudaGraphNodeParams sp = {};
+    sp.type = cudaGraphNodeTypeConditional;
+    sp.conditional.handle = h_step;
+    sp.conditional.type = cudaGraphCondTypeSwitch;
+    sp.conditional.size = kSchedOut;
+    cudaGraphNode_t switch_node = nullptr;
+    GCU_CUDA(cudaGraphAddNode(&switch_node, body, &decide_node, 1, &sp), "cudaGraphAddNode (switch)");
+    cudaGraph_t* branch = sp.conditional.phGraph_out;
+    GCU_TRY(capture_into(dev, branch[kPushWarp], [&]() -> Error {
+        GCU_LAUNCH(dev, "bfs_topdown_warp", bfs_topdown_warp_loop_kernel, wgrid, kTdThreads, 0, g.offsets.ptr,
+                   g.targets.ptr, w.queue[0].ptr, w.queue[1].ptr, w.dist.ptr, w.visited.ptr, w.counters.ptr, st);
+        return ok();
+    }));
+    GCU_TRY(capture_into(dev, branch[kPushBalanced], [&]() -> Error {
+        GCU_LAUNCH(dev, "bfs_queue_degrees", bfs_queue_degrees_loop_kernel, vgrid, 256, 0, g.offsets.ptr,
+                   w.queue[0].ptr, w.queue[1].ptr, st, w.degree_scan.ptr);
+        GCU_TRY(exclusive_scan_u32_device_n(dev, w.degree_scan.ptr, w.degree_scan.ptr, n_ptr, V,
+                                            w.loop_scan_sums.ptr));
+        GCU_LAUNCH(dev, "bfs_topdown", bfs_topdown_loop_kernel, td_grid, kTdThreads, 0, g.offsets.ptr, g.targets.ptr,
+                   w.queue[0].ptr, w.queue[1].ptr, w.degree_scan.ptr, w.dist.ptr, w.visited.ptr, w.counters.ptr, st);
+        return ok();
+    }));
+    GCU_TRY(capture_into(dev, branch[kPull], [&]() -> Error {
+        GCU_LAUNCH(dev, "bfs_bitmap_clear", bfs_bitmap_clear_loop_kernel, vgrid, 256, 0, w.bitmap[0].ptr,
+                   w.bitmap[1].ptr, words, st);
+        GCU_LAUNCH(dev, "bfs_queue_to_bitmap", bfs_queue_to_bitmap_loop_kernel, vgrid, 256, 0, w.queue[0].ptr,
+                   w.queue[1].ptr, w.bitmap[0].ptr, w.bitmap[1].ptr, st);
+        GCU_LAUNCH(dev, "bfs_bottomup", bfs_bottomup_loop_kernel, bu_grid, kBuThreads, 0, g.offsets.ptr,
+                   g.targets.ptr, V, w.bitmap[0].ptr, w.bitmap[1].ptr, w.visited.ptr, w.dist.ptr, w.queue[0].ptr,
+                   w.queue[1].ptr, w.counters.ptr, st);
+        return ok();
+    }));
+    cudaGraphExec_t exec = nullptr;
+    GCU_CUDA(cudaGraphInstantiate(&exec, graph, 0), "cudaGraphInstantiate");
+    w.loop_graph = graph;
+    owner.g = nullptr;
+    w.loop_exec = exec;
+    w.loop_net = net;
+    return ok();
+}
+
+// One search through the loop graph; the final state gives reachable and
+// max_depth.
+Error run_loop(GraphImpl& g, BfsWork& w, uint32_t source, BfsDevState* final_state) {
+    DeviceImpl& dev = *g.dev;
+    const uint64_t words = ceil_div_u64(g.num_nodes, 32);
+    GCU_CUDA(cudaMemsetAsync(w.dist.ptr, 0xFF, sizeof(int32_t) * g.num_nodes, dev.stream), "memset");
+    GCU_CUDA(cudaMemsetAsync(w.visited.ptr, 0, sizeof(uint32_t) * words, dev.stream), "memset");
+    GCU_LAUNCH(dev, "bfs_init", bfs_loop_init_kernel, 1, 32, 0, g.offsets.ptr, source, w.dist.ptr, w.visited.ptr,
+               w.queue[0].ptr, w.counters.ptr, w.loop_state.ptr);
+    dev.launches.fetch_add(1, std::memory_order_relaxed);
+    GCU_CUDA(cudaGraphLaunch(w.loop_exec, dev.stream), "cudaGraphLaunch");
+    GCU_CUDA(cudaMemcpyAsync(w.host_loop_state, w.loop_state.ptr, sizeof(BfsDevState), cudaMemcpyDeviceToHost,
+                             dev.stream),
+             "copy");
+    GCU_TRY(dev.sync());
+    *final_state = *w.host_loop_state;
+    return ok();
+}
+
 uint64_t mix64(uint64_t z) {
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
@@ -480,6 +840,28 @@ Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reac
     const __nv_bfloat16* net = reinterpret_cast<const __nv_bfloat16*>(dev.schedule);
     DegreeStats stats;
     if (net) GCU_TRY(degree_stats(g, &stats));
+
+    if (dev.bfs_device_loop && !dev.kernel_timing && !w.loop_unavailable) {
+        if (!w.loop_exec || w.loop_net != static_cast<const void*>(net)) {
+            // A driver that cannot build the conditional graph leaves the
+            // search to the host-driven loop below (same kernels, same result).
+            if (!build_loop_graph(g, w).ok()) w.loop_unavailable = true;
+        }
+        if (w.loop_exec) {
+            BfsDevState fin{};
+            GCU_TRY(run_loop(g, w, source, &fin));
+            if (fin.failed) return kernel_error("BFS level loop stopped on an impossible state");
+            if (host_distances) {
+                GCU_CUDA(cudaMemcpyAsync(host_distances, w.dist.ptr, sizeof(int32_t) * g.num_nodes,
+                                         cudaMemcpyDeviceToHost, dev.stream),
+                         "copy distances to host");
+                GCU_TRY(dev.sync());
+            }
+            *reachable = fin.reached;
+            *max_depth = fin.level;
+            return ok();
+        }
+    }
 
     GCU_TRY(start_run(g, w, source));
     if (net)

@@ -95,6 +95,9 @@ struct DeviceImpl {
 
     std::atomic<uint64_t> launches{0};
     bool kernel_timing = false;
+    // BFS runs its level loop on the device (one CUDA graph per search)
+    // unless this is off or per-kernel timing is on.
+    bool bfs_device_loop = true;
     std::mutex stats_mu;
     std::map<std::string, KernelStat> stats;
     struct Pending {
@@ -242,6 +245,12 @@ Error truss_decomposition(GraphImpl& g, uint32_t* host_truss, uint32_t* max_trus
 // Exclusive scan of u32 counts into u32 offsets (out has n + 1 entries);
 // returns the total through the device (out[n]).
 Error exclusive_scan_u32(DeviceImpl& dev, const uint32_t* d_in, uint32_t* d_out, uint64_t n);
+// The same scan with its length n = *d_n read on the device (n <= max_n),
+// for launch sequences captured into a CUDA graph: out[0..n) = exclusive
+// prefix, out[n] = total. tile_sums holds scan_device_n_tiles(max_n) values.
+Error exclusive_scan_u32_device_n(DeviceImpl& dev, const uint32_t* d_in, uint32_t* d_out, const uint32_t* d_n,
+                                  uint64_t max_n, uint32_t* tile_sums);
+uint64_t scan_device_n_tiles(uint64_t max_n);
 
 // Stable LSD radix sort of n 64-bit keys by bits [low_bit, high_bit), 8 per
 // pass, ping-ponging between keys and tmp; *sorted is whichever holds the result.

@@ -303,6 +303,11 @@ GCU_API void gcu_device_set_kernel_timing(gcu_device* dev, int on) {
     dev->impl->kernel_timing = on != 0;
 }
 
+GCU_API void gcu_device_set_bfs_device_loop(gcu_device* dev, int on) {
+    if (!dev) return;
+    dev->impl->bfs_device_loop = on != 0;
+}
+
 GCU_API size_t gcu_device_kernel_stats(gcu_device* dev, char* buf, size_t buflen) {
     if (!dev) return 0;
     DeviceImpl& d = *dev->impl;

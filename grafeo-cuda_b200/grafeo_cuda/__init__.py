@@ -142,6 +142,11 @@ class GpuDevice:
     def set_kernel_timing(self, on: bool) -> None:
         lib.gcu_device_set_kernel_timing(self._h, 1 if on else 0)
 
+    def set_bfs_device_loop(self, on: bool) -> None:
+        """BFS level loop on the device (default) or driven from the host;
+        the host drives it whenever per-kernel timing is on."""
+        lib.gcu_device_set_bfs_device_loop(self._h, 1 if on else 0)
+
     def kernel_stats(self) -> dict:
         n = lib.gcu_device_kernel_stats(self._h, None, 0)
         buf = C.create_string_buffer(int(n))

@@ -36,6 +36,7 @@ SIGNATURES = {
     "gcu_device_timer_stop": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "gcu_device_launch_count": (C.c_uint64, [C.c_void_p]),
     "gcu_device_set_kernel_timing": (None, [C.c_void_p, C.c_int]),
+    "gcu_device_set_bfs_device_loop": (None, [C.c_void_p, C.c_int]),
     "gcu_device_kernel_stats": (C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "gcu_device_reset_stats": (None, [C.c_void_p]),
     "gcu_validate_csr": (C.c_int, [u32p, C.c_size_t, u32p, C.c_size_t]),

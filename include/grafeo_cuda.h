@@ -82,6 +82,13 @@ GCU_API uint64_t gcu_device_launch_count(const gcu_device* dev);
 /* When on, every kernel launch is bracketed by CUDA events and its device time
  * is accumulated per kernel name. */
 GCU_API void gcu_device_set_kernel_timing(gcu_device* dev, int on);
+/* BFS level loop on the device (default, on = 1): a search is one CUDA-graph
+ * launch whose WHILE node runs decide + step until the frontier is empty, with
+ * no host round trip per level. on = 0 (or per-kernel timing on) drives the
+ * levels from the host, reading the counters back after each step. Results
+ * are the same either way. No reference counterpart (bfs.rs:42-131 syncs
+ * every level). */
+GCU_API void gcu_device_set_bfs_device_loop(gcu_device* dev, int on);
 /* Writes per-kernel statistics as JSON {"name": [launches, total_ms], ...}
  * into buf (always NUL-terminated) and returns the full length needed. */
 GCU_API size_t gcu_device_kernel_stats(gcu_device* dev, char* buf, size_t buflen);
