@@ -291,10 +291,33 @@ def main(argv=None) -> int:
     t.add_argument("--out", default=DEFAULT_WEIGHTS)
     t.add_argument("--report", default=None, help="write the evaluation JSON here too")
     t.add_argument("--save-traces", default=None, help="write the training and held-out traces (.npz)")
+    e = sub.add_parser("eval", help="evaluate the shipped (or given) network on held-out graphs, no training")
+    e.add_argument("--heldout", type=int, default=200)
+    e.add_argument("--timed", type=int, default=30)
+    e.add_argument("--sources", type=int, default=2)
+    e.add_argument("--scale-min", type=int, default=16)
+    e.add_argument("--scale-max", type=int, default=22)
+    e.add_argument("--seed", type=int, default=4)
+    e.add_argument("--weights", default=DEFAULT_WEIGHTS)
+    e.add_argument("--report", default=None)
     a = ap.parse_args(argv)
 
     dev = G.GpuDevice(0)
     log = lambda msg: print(msg, flush=True)  # noqa: E731
+    if a.cmd == "eval":
+        w16 = load(a.weights)
+        held_specs = corpus(a.heldout, HELDOUT_SEED_BASE + a.seed, (a.scale_min, a.scale_max))
+        held = collect(dev, held_specs, a.sources, explore=False, log=log)
+        report = {"weights": os.path.basename(a.weights), "margin_log2": MARGIN_LOG2,
+                  "heldout": {"graphs": a.heldout, "decisions": int(len(held["valid"])),
+                              "trace_gain": trace_gain(dev, w16, held)}}
+        if a.timed:
+            report["heldout"]["timed"] = timed_runs(dev, w16, held_specs[: a.timed])
+        log(json.dumps(report, indent=1))
+        if a.report:
+            with open(a.report, "w") as fh:
+                json.dump(report, fh, indent=1)
+        return 0
     scales = (a.scale_min, a.scale_max)
     t0 = time.time()
     train_specs = corpus(a.graphs, a.seed, scales)
