@@ -61,6 +61,11 @@ constexpr int kMaxPhases = 16;
 constexpr int kRowsPerGroup = 2;      // rows a lane group works on in lockstep
 constexpr int kUnroll = 2;            // steps per loop trip: kRowsPerGroup * kUnroll loads in flight
 constexpr int kRowCtasPerSm = 8;      // persistent CTAs of the row kernel per SM
+// Hub cache: every CTA of the row kernel copies the contributions of the new
+// ids [0, kHubEntries) (the highest-degree vertices, which take the largest
+// share of the gathers) into shared memory at the start of a launch and
+// gathers below that bound from there; 0 turns it off.
+constexpr uint32_t kHubEntries = 0;
 
 enum : uint32_t { kPhaseLong = 0, kPhaseGroup = 1, kPhaseEmpty = 2 };
 
@@ -342,7 +347,15 @@ __device__ __forceinline__ double group_sum(double v, uint32_t log2g) {
 // evenly over the warps, the warps in flight read one contiguous window of
 // the CSR, and no block barrier ties the warps of a CTA together inside the
 // loop. 8 CTAs of 256 threads per SM.
-__global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
+// Contribution of source t: from the shared hub copy when t < kHubEntries
+// (every target is below V, so such a t is inside the copied min(V,
+// kHubEntries) entries), else a gather from global memory.
+__device__ __forceinline__ float gather_contrib(const float* s_hub, const float* __restrict__ contrib, uint32_t t) {
+    if (kHubEntries > 0 && t < kHubEntries) return s_hub[t];
+    return __ldg(contrib + t);
+}
+
+__global__ void __launch_bounds__(kPrThreads, kRowCtasPerSm) pr_rows_kernel(
     const uint32_t* __restrict__ poff, const uint32_t* __restrict__ ptgt, const float* __restrict__ rank_in,
     const float* __restrict__ contrib_in, float* __restrict__ rank_out, float* __restrict__ contrib_out,
     const uint32_t* __restrict__ outdeg, const float* __restrict__ tele, uint32_t V, double base, double damp,
@@ -362,6 +375,11 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
         s_mass[1] = state->dangling / static_cast<double>(V);
     }
     if (threadIdx.x < 2 * kWarps) s_sum[threadIdx.x] = 0;
+    extern __shared__ float s_hub[];  // kHubEntries floats (dynamic shared memory)
+    if (kHubEntries > 0) {
+        const uint32_t hub = V < kHubEntries ? V : kHubEntries;
+        for (uint32_t i = threadIdx.x; i < hub; i += blockDim.x) s_hub[i] = __ldg(contrib_in + i);
+    }
     __syncthreads();
     const uint32_t total_warps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t first_unit = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -385,11 +403,11 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
                     for (int q = 0; q < 8; ++q) t[q] = ld_stream(ptgt + j + q * 32);
                     float c[8];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) c[q] = __ldg(contrib_in + t[q]);
+                    for (int q = 0; q < 8; ++q) c[q] = gather_contrib(s_hub, contrib_in, t[q]);
 #pragma unroll
                     for (int q = 0; q < 8; ++q) kahan_add(acc, comp, c[q]);
                 }
-                for (; j < s1; j += 32) kahan_add(acc, comp, __ldg(contrib_in + ld_stream(ptgt + j)));
+                for (; j < s1; j += 32) kahan_add(acc, comp, gather_contrib(s_hub, contrib_in, ld_stream(ptgt + j)));
                 const double part = warp_sum(static_cast<double>(acc) - static_cast<double>(comp));
                 if (lane == 0) seg_partial[b - ph.first_block] = part;
             } else if (ph.kind == kPhaseGroup) {
@@ -434,7 +452,7 @@ __global__ void __launch_bounds__(kPrThreads, 8) pr_rows_kernel(
                     for (int u = 0; u < kUnroll; ++u) {
 #pragma unroll
                         for (int q = 0; q < kRowsPerGroup; ++q) {
-                            if (t[u][q] != 0xFFFFFFFFu) kahan_add(acc[q], comp[q], __ldg(contrib_in + t[u][q]));
+                            if (t[u][q] != 0xFFFFFFFFu) kahan_add(acc[q], comp[q], gather_contrib(s_hub, contrib_in, t[u][q]));
                         }
                     }
                 }
@@ -660,6 +678,10 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
     p.row_ctas = std::max<uint32_t>(
         1, std::min<uint32_t>(ceil_div_u64(blocks, kPrThreads / 32), static_cast<uint32_t>(dev.sm_count) * kRowCtasPerSm));
 
+    if (kHubEntries * sizeof(float) > 48 * 1024)
+        GCU_CUDA(cudaFuncSetAttribute(pr_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(kHubEntries * sizeof(float))),
+                 "cudaFuncSetAttribute");
     p.fin_blocks = static_cast<uint32_t>(
         std::max<uint64_t>({1, ceil_div_u64(p.long_rows, 256), ceil_div_u64(p.row_ctas, kFinSlice)}));
 
@@ -748,7 +770,8 @@ Error pagerank_ex(GraphImpl& g, bool directed, const float* tele_host, float dam
             const uint32_t it = launched + i;
             const int in = it & 1, out = in ^ 1;
             err = [&]() -> Error {
-                GCU_LAUNCH(dev, "pr_rows", pr_rows_kernel, p.row_ctas, kPrThreads, 0, p.poff.ptr, p.ptgt.ptr,
+                GCU_LAUNCH(dev, "pr_rows", pr_rows_kernel, p.row_ctas, kPrThreads, kHubEntries * sizeof(float),
+                           p.poff.ptr, p.ptgt.ptr,
                            ranks[in], contrib[in], ranks[out], contrib[out], outdeg, d_tele, V, base, damp,
                            p.state.ptr, p.sched, p.units.ptr, p.seg_partial.ptr, p.row_partials.ptr);
                 GCU_LAUNCH(dev, "pr_finish", pr_finish_kernel, p.fin_blocks, 256, 0, p.poff.ptr, p.long_rows,
