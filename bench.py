@@ -504,6 +504,7 @@ def run_ours(args, d: Dist) -> dict | None:
             algos[name] = symmetric_block(gg, gg.to_csr(), dev, name + ("_seed2" if name == "rmat22" else "_seed3"),
                                           harness, decomposition=False, sweep=True, pagerank=True)
             del gg
+        algos["rmat14"] = small_config_block(dev, harness)
         line["algorithms"] = algos
         line["harness"] = harness
         if args.save:
@@ -611,6 +612,37 @@ def symmetric_block(g, csr, dev, dataset: str, harness: list, decomposition: boo
                                       "max_trussness": td["max_trussness"], "rounds": td["rounds"], **stats(runs)}
         harness.append(harness_record(dataset, "gpu_truss_decomposition", V, E, transfer_s, runs, float(E), dev.name,
                                       {"max_trussness": td["max_trussness"], "rounds": td["rounds"]}))
+    return out
+
+
+def small_config_block(dev, harness: list) -> dict:
+    """The plain method at small size: R-MAT 14 seed 1; PageRank 20
+    iterations (tol 1e-6), BFS from vertex 0, triangles, k-truss k = 4;
+    device times, RUNS runs each."""
+    import grafeo_cuda as G
+
+    g = G.GpuGraph.generate_rmat(dev, 14, EDGE_FACTOR, *RMAT_ABC, seed=1)
+    V, E = g.num_nodes, g.num_edges
+    out = {"vertices": V, "csr_entries": E}
+    runs, r = timed(dev, lambda: g.pagerank_array(DAMPING, 20, 1e-6, copy_result=False))
+    out["pagerank"] = {"iterations": r["iterations"], "ms_median": round(statistics.median(runs), 4),
+                       "gbs": round(pr_bytes(V, E) * r["iterations"] / (statistics.median(runs) / 1e3) / 1e9, 1)}
+    harness.append(harness_record("rmat14_seed1", "gpu_pagerank", V, E, 0.0, runs, float(E) * r["iterations"],
+                                  dev.name, {"iterations": r["iterations"]}))
+    runs, r = timed(dev, lambda: g.bfs_array(0, copy_result=False))
+    out["bfs_from_0"] = {"reachable": r["reachable"], "max_depth": r["max_depth"],
+                         "ms_median": round(statistics.median(runs), 4)}
+    harness.append(harness_record("rmat14_seed1", "gpu_bfs", V, E, 0.0, runs, float(E), dev.name,
+                                  {"source_node": 0, "reachable_nodes": r["reachable"], "max_depth": r["max_depth"]}))
+    runs, r = timed(dev, g.triangle_count)
+    out["triangle_count"] = {"triangles": r["total_triangles"], "ms_median": round(statistics.median(runs), 4)}
+    harness.append(harness_record("rmat14_seed1", "gpu_triangle_count", V, E, 0.0, runs, float(E), dev.name,
+                                  {"triangles": r["total_triangles"]}))
+    runs, r = timed(dev, lambda: g.k_truss_array(4))
+    out["k_truss_4"] = {"edges": int(len(r["edges"])), "rounds": r["iterations"],
+                        "ms_median": round(statistics.median(runs), 4)}
+    harness.append(harness_record("rmat14_seed1", "gpu_ktruss", V, E, 0.0, runs, float(E), dev.name,
+                                  {"k": 4, "truss_edges": int(len(r["edges"])), "iterations": r["iterations"]}))
     return out
 
 
