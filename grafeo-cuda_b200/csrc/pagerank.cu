@@ -20,8 +20,8 @@
 //    of 2^(c-1) lanes per row (1 to 32); a group works on 2 rows in lockstep,
 //    2 steps per trip (a row of class c has fewer than 2g entries, so a third
 //    step would always be masked below class 6), so every lane keeps 4
-//    independent loads in flight within 32 registers (8 CTAs per SM,
-//    persistent); consecutive groups read
+//    independent loads in flight within 32 registers (2 CTAs of 1024
+//    threads per SM, persistent); consecutive groups read
 //    consecutive rows (coalesced), and there is no search, staging, barrier or
 //    carry. Rows of 1024 or more entries are split into 1024-entry segments,
 //    one warp each, and their partial sums are added in segment order by the
@@ -52,7 +52,12 @@
 
 namespace gcu {
 
-constexpr int kPrThreads = 256;
+// Two CTAs of 1024 threads per SM: the 32 warps of a CTA hold consecutive
+// work units, so an SM works on two contiguous windows of rows at a time
+// instead of eight; their gathers share more L1 lines (R-MAT 24 directed:
+// 1.871 -> 1.771 ms per iteration against 8 CTAs of 256, R-MAT 22: 0.443 ->
+// 0.439 ms; same ranks bit for bit).
+constexpr int kPrThreads = 1024;
 constexpr int kDegClasses = 33;       // class 0: degree 0; class c: degree in [2^(c-1), 2^c)
 constexpr int kLongClass = 11;        // degree >= 1024
 constexpr uint32_t kSegment = 1024;   // entries per long-row segment (one warp)
@@ -60,11 +65,15 @@ constexpr int kClassBlock = 1024;     // vertices per block of the class partiti
 constexpr int kMaxPhases = 16;
 constexpr int kRowsPerGroup = 2;      // rows a lane group works on in lockstep
 constexpr int kUnroll = 2;            // steps per loop trip: kRowsPerGroup * kUnroll loads in flight
-constexpr int kRowCtasPerSm = 8;      // persistent CTAs of the row kernel per SM
+constexpr int kRowCtasPerSm = 2;      // persistent CTAs of the row kernel per SM
 // Hub cache: every CTA of the row kernel copies the contributions of the new
 // ids [0, kHubEntries) (the highest-degree vertices, which take the largest
 // share of the gathers) into shared memory at the start of a launch and
-// gathers below that bound from there; 0 turns it off.
+// gathers below that bound from there; 0 turns it off. Measured on B200
+// (same ranks bit for bit): 16K entries (40 % of the gathers at R-MAT 22) with
+// two 768-thread CTAs per SM ran R-MAT 22 2.6 % faster than the plain 8 x 256
+// kernel but R-MAT 24 no faster than two 1024-thread CTAs without it; 24K and
+// 32K entries ran slower (the carve-out shrinks L1). Off.
 constexpr uint32_t kHubEntries = 0;
 
 enum : uint32_t { kPhaseLong = 0, kPhaseGroup = 1, kPhaseEmpty = 2 };
@@ -346,7 +355,8 @@ __device__ __forceinline__ double group_sum(double v, uint32_t log2g) {
 // degree class, or 32 rows without entries). Every phase's units are spread
 // evenly over the warps, the warps in flight read one contiguous window of
 // the CSR, and no block barrier ties the warps of a CTA together inside the
-// loop. 8 CTAs of 256 threads per SM.
+// loop. 2 CTAs of 1024 threads per SM.
+
 // Contribution of source t: from the shared hub copy when t < kHubEntries
 // (every target is below V, so such a t is inside the copied min(V,
 // kHubEntries) entries), else a gather from global memory.
