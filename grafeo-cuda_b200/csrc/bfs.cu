@@ -496,11 +496,16 @@ __global__ void __launch_bounds__(kTdThreads) bfs_topdown_warp_loop_kernel(
                       ctr, st->level + 1);
 }
 
+// Also sets the IF node that picks the scan: three kernels above
+// kScanOneLaunchMax frontier vertices, one below.
 __global__ void bfs_queue_degrees_loop_kernel(const uint32_t* __restrict__ offsets, const uint32_t* queue0,
                                               const uint32_t* queue1, const BfsDevState* __restrict__ st,
-                                              uint32_t* __restrict__ deg) {
+                                              uint32_t* __restrict__ deg, int set_big,
+                                              cudaGraphConditionalHandle h_big) {
     const uint32_t* queue = st->cur ? queue1 : queue0;
     const uint32_t n = st->frontier_q;
+    if (set_big && blockIdx.x == 0 && threadIdx.x == 0)
+        cudaGraphSetConditional(h_big, n > kScanOneLaunchMax ? 1u : 0u);
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         const uint32_t u = queue[i];
@@ -685,10 +690,11 @@ void advance(BfsState& st, const BfsCounters& c, bool first, int variant, uint64
 }
 
 // Captures the launches `f` makes on the device stream into `target` (a
-// conditional node's body graph).
+// conditional node's body graph), after the node `after` when given.
 template <class F>
-Error capture_into(DeviceImpl& dev, cudaGraph_t target, F&& f) {
-    GCU_CUDA(cudaStreamBeginCaptureToGraph(dev.stream, target, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal),
+Error capture_into(DeviceImpl& dev, cudaGraph_t target, F&& f, const cudaGraphNode_t* after = nullptr) {
+    GCU_CUDA(cudaStreamBeginCaptureToGraph(dev.stream, target, after, nullptr, after ? 1 : 0,
+                                           cudaStreamCaptureModeThreadLocal),
              "cudaStreamBeginCaptureToGraph");
     const Error e = f();
     cudaGraph_t captured = nullptr;
@@ -776,15 +782,49 @@ Error build_loop_graph(GraphImpl& g, BfsWork& w) {
                    g.targets.ptr, w.queue[0].ptr, w.queue[1].ptr, w.dist.ptr, w.visited.ptr, w.counters.ptr, st);
         return ok();
     }));
-    GCU_TRY(capture_into(dev, branch[kPushBalanced], [&]() -> Error {
-        GCU_LAUNCH(dev, "bfs_queue_degrees", bfs_queue_degrees_loop_kernel, vgrid, 256, 0, g.offsets.ptr,
-                   w.queue[0].ptr, w.queue[1].ptr, st, w.degree_scan.ptr);
-        GCU_TRY(exclusive_scan_u32_device_n(dev, w.degree_scan.ptr, w.degree_scan.ptr, n_ptr, V,
-                                            w.loop_scan_sums.ptr));
+    // Balanced push: degrees (which set the scan's IF), IF(n > 8192) { three-kernel
+    // scan } ELSE { one-kernel scan }, expand. Graphs of at most 8192
+    // vertices only ever take the one-kernel scan: no IF node.
+    cudaGraph_t balanced = branch[kPushBalanced];
+    const bool big = V > kScanOneLaunchMax;
+    cudaGraphConditionalHandle h_big = 0;
+    if (big)
+        GCU_CUDA(cudaGraphConditionalHandleCreate(&h_big, balanced, 0, 0), "cudaGraphConditionalHandleCreate");
+    auto launch_expand = [&]() -> Error {
         GCU_LAUNCH(dev, "bfs_topdown", bfs_topdown_loop_kernel, td_grid, kTdThreads, 0, g.offsets.ptr, g.targets.ptr,
                    w.queue[0].ptr, w.queue[1].ptr, w.degree_scan.ptr, w.dist.ptr, w.visited.ptr, w.counters.ptr, st);
         return ok();
+    };
+    GCU_TRY(capture_into(dev, balanced, [&]() -> Error {
+        GCU_LAUNCH(dev, "bfs_queue_degrees", bfs_queue_degrees_loop_kernel, vgrid, 256, 0, g.offsets.ptr,
+                   w.queue[0].ptr, w.queue[1].ptr, st, w.degree_scan.ptr, big ? 1 : 0, h_big);
+        if (big) return ok();
+        GCU_TRY(exclusive_scan_u32_device_n(dev, w.degree_scan.ptr, w.degree_scan.ptr, n_ptr, V,
+                                            w.loop_scan_sums.ptr, ScanLaunches::kOneTile));
+        return launch_expand();
     }));
+    if (big) {
+        cudaGraphNode_t degrees_node = nullptr;
+        nodes = 1;
+        GCU_CUDA(cudaGraphGetNodes(balanced, &degrees_node, &nodes), "cudaGraphGetNodes");
+        if (nodes != 1) return kernel_error("BFS loop graph: unexpected balanced branch");
+        cudaGraphNodeParams ip = {};
+        ip.type = cudaGraphNodeTypeConditional;
+        ip.conditional.handle = h_big;
+        ip.conditional.type = cudaGraphCondTypeIf;
+        ip.conditional.size = 2;
+        cudaGraphNode_t if_node = nullptr;
+        GCU_CUDA(cudaGraphAddNode(&if_node, balanced, &degrees_node, 1, &ip), "cudaGraphAddNode (if)");
+        GCU_TRY(capture_into(dev, ip.conditional.phGraph_out[0], [&]() -> Error {
+            return exclusive_scan_u32_device_n(dev, w.degree_scan.ptr, w.degree_scan.ptr, n_ptr, V,
+                                               w.loop_scan_sums.ptr, ScanLaunches::kMultiTile);
+        }));
+        GCU_TRY(capture_into(dev, ip.conditional.phGraph_out[1], [&]() -> Error {
+            return exclusive_scan_u32_device_n(dev, w.degree_scan.ptr, w.degree_scan.ptr, n_ptr, V,
+                                               w.loop_scan_sums.ptr, ScanLaunches::kOneTile);
+        }));
+        GCU_TRY(capture_into(dev, balanced, launch_expand, &if_node));
+    }
     GCU_TRY(capture_into(dev, branch[kPull], [&]() -> Error {
         GCU_LAUNCH(dev, "bfs_bitmap_clear", bfs_bitmap_clear_loop_kernel, vgrid, 256, 0, w.bitmap[0].ptr,
                    w.bitmap[1].ptr, words, st);

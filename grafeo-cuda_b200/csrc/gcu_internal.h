@@ -248,8 +248,13 @@ Error exclusive_scan_u32(DeviceImpl& dev, const uint32_t* d_in, uint32_t* d_out,
 // The same scan with its length n = *d_n read on the device (n <= max_n),
 // for launch sequences captured into a CUDA graph: out[0..n) = exclusive
 // prefix, out[n] = total. tile_sums holds scan_device_n_tiles(max_n) values.
+// Lengths up to kScanOneLaunchMax take one kernel, longer ones three; each
+// kernel returns at once when the length is not its case, and `which` leaves
+// out the launches a caller's graph never needs (an IF node on the length).
+constexpr uint64_t kScanOneLaunchMax = 8192;
+enum class ScanLaunches { kBoth, kOneTile, kMultiTile };
 Error exclusive_scan_u32_device_n(DeviceImpl& dev, const uint32_t* d_in, uint32_t* d_out, const uint32_t* d_n,
-                                  uint64_t max_n, uint32_t* tile_sums);
+                                  uint64_t max_n, uint32_t* tile_sums, ScanLaunches which = ScanLaunches::kBoth);
 uint64_t scan_device_n_tiles(uint64_t max_n);
 
 // Stable LSD radix sort of n 64-bit keys by bits [low_bit, high_bit), 8 per

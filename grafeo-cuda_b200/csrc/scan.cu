@@ -257,12 +257,15 @@ __global__ void __launch_bounds__(kScanThreads) scan_tiles_dn_kernel(const uint3
 
 uint64_t scan_device_n_tiles(uint64_t max_n) { return std::max<uint64_t>(1, ceil_div_u64(max_n, kScanTile)); }
 
+static_assert(kScanTile == kScanOneLaunchMax, "one-launch scan size");
+
 Error exclusive_scan_u32_device_n(DeviceImpl& dev, const uint32_t* d_in, uint32_t* d_out, const uint32_t* d_n,
-                                  uint64_t max_n, uint32_t* tile_sums) {
+                                  uint64_t max_n, uint32_t* tile_sums, ScanLaunches which) {
     const unsigned grid = static_cast<unsigned>(
         std::max<uint64_t>(1, std::min<uint64_t>(scan_device_n_tiles(max_n), static_cast<uint64_t>(dev.sm_count) * 2)));
-    GCU_LAUNCH(dev, "scan_one_tile", scan_one_tile_dn_kernel, 1, kScanThreads, 0, d_in, d_n, d_out);
-    if (max_n > static_cast<uint64_t>(kScanTile)) {
+    if (which != ScanLaunches::kMultiTile)
+        GCU_LAUNCH(dev, "scan_one_tile", scan_one_tile_dn_kernel, 1, kScanThreads, 0, d_in, d_n, d_out);
+    if (which != ScanLaunches::kOneTile && max_n > static_cast<uint64_t>(kScanTile)) {
         GCU_LAUNCH(dev, "scan_tile_sums", scan_tile_sums_dn_kernel, grid, kScanThreads, 0, d_in, d_n, tile_sums);
         GCU_LAUNCH(dev, "scan_tile_prefix", scan_tile_prefix_dn_kernel, 1, kScanThreads, 0, tile_sums, d_n, d_out);
         GCU_LAUNCH(dev, "scan_tiles", scan_tiles_dn_kernel, grid, kScanThreads, 0, d_in, d_n, tile_sums, d_out);
