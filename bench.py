@@ -281,7 +281,8 @@ def workload_config(scale: int, V: int, E_pull: int, n_dangling: int, world: int
         "csr_entries": E_pull,
         "dangling_vertices": n_dangling,
         "bytes_per_iteration": pr_bytes(V, E_pull),
-        "l2": "inputs larger than L2 (in-CSR %.2f GB > 126 MB)" % ((4 * (V + 1) + 4 * E_pull) / 1e9),
+        "l2": ("inputs larger than L2 (in-CSR %.2f GB > 126 MB)" if 4 * (V + 1) + 4 * E_pull > 126e6
+               else "inputs smaller than L2 (in-CSR %.2f GB)") % ((4 * (V + 1) + 4 * E_pull) / 1e9),
         "parallelism": f"replicas x{world}",
     }
 
