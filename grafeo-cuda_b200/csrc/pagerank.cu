@@ -75,6 +75,8 @@ constexpr int kRowCtasPerSm = 2;      // persistent CTAs of the row kernel per S
 // kernel but R-MAT 24 no faster than two 1024-thread CTAs without it; 24K and
 // 32K entries ran slower (the carve-out shrinks L1). Off.
 constexpr uint32_t kHubEntries = 0;
+// Load the next group-phase unit's row offsets while working on this one.
+constexpr bool kPrefetchRows = false;
 
 enum : uint32_t { kPhaseLong = 0, kPhaseGroup = 1, kPhaseEmpty = 2 };
 
@@ -357,6 +359,31 @@ __device__ __forceinline__ double group_sum(double v, uint32_t log2g) {
 // the CSR, and no block barrier ties the warps of a CTA together inside the
 // loop. 2 CTAs of 1024 threads per SM.
 
+// Phase of work unit b.
+__device__ __forceinline__ uint32_t unit_phase(const PrSchedule& sched, uint32_t b) {
+    uint32_t pi = 0;
+    while (pi + 1 < sched.nphases && sched.phase[pi + 1].first_block <= b) ++pi;
+    return pi;
+}
+
+// Row bounds of this lane's kRowsPerGroup rows in work unit b of a group
+// phase (0, 0 past the phase's last row).
+__device__ __forceinline__ void unit_rows(const PrPhase& ph, uint32_t b, unsigned lane,
+                                          const uint32_t* __restrict__ poff, uint32_t* rs, uint32_t* re) {
+    const uint32_t groups = 32u >> ph.log2g, group = lane >> ph.log2g;
+    const uint32_t first = ph.row_begin + (b - ph.first_block) * groups * kRowsPerGroup;
+#pragma unroll
+    for (int q = 0; q < kRowsPerGroup; ++q) {
+        const uint32_t row = first + q * groups + group;
+        rs[q] = 0;
+        re[q] = 0;
+        if (row < ph.row_end) {
+            rs[q] = poff[row];
+            re[q] = poff[row + 1];
+        }
+    }
+}
+
 // Contribution of source t: from the shared hub copy when t < kHubEntries
 // (every target is below V, so such a t is inside the copied min(V,
 // kHubEntries) entries), else a gather from global memory.
@@ -395,9 +422,23 @@ __global__ void __launch_bounds__(kPrThreads, kRowCtasPerSm) pr_rows_kernel(
     const uint32_t first_unit = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     unsigned long long my_diff = 0, my_dangle = 0;
     {
-        for (uint32_t b = first_unit; b < sched.total_blocks; b += total_warps) {
-            uint32_t pi = 0;
-            while (pi + 1 < sched.nphases && sched.phase[pi + 1].first_block <= b) ++pi;
+        // The row bounds of the next group-phase unit are loaded while this
+        // unit is worked on: a unit's loads form a chain (row offsets, then
+        // targets, then gathers), and most lanes finish a unit in one trip,
+        // so the offsets' latency would otherwise be paid in full each time.
+        uint32_t b = first_unit;
+        uint32_t pi = 0, rs[kRowsPerGroup] = {}, re[kRowsPerGroup] = {};
+        if (b < sched.total_blocks) {
+            pi = unit_phase(sched, b);
+            if (sched.phase[pi].kind == kPhaseGroup) unit_rows(sched.phase[pi], b, lane, poff, rs, re);
+        }
+        while (b < sched.total_blocks) {
+            const uint32_t nb = b + total_warps;
+            uint32_t npi = 0, nrs[kRowsPerGroup] = {}, nre[kRowsPerGroup] = {};
+            if (kPrefetchRows && nb < sched.total_blocks) {
+                npi = unit_phase(sched, nb);
+                if (sched.phase[npi].kind == kPhaseGroup) unit_rows(sched.phase[npi], nb, lane, poff, nrs, nre);
+            }
             const PrPhase ph = sched.phase[pi];
             if (ph.kind == kPhaseLong) {
                 // One segment of a long row: 32 entries per lane, 8 loads in flight.
@@ -429,19 +470,9 @@ __global__ void __launch_bounds__(kPrThreads, kRowCtasPerSm) pr_rows_kernel(
                 const uint32_t groups = 32u >> log2g;
                 const uint32_t group = lane >> log2g, lig = lane & (g - 1);
                 const uint32_t first = ph.row_begin + (b - ph.first_block) * groups * kRowsPerGroup;
-                uint32_t rs[kRowsPerGroup], re[kRowsPerGroup];
                 uint32_t longest = 0;
 #pragma unroll
-                for (int q = 0; q < kRowsPerGroup; ++q) {
-                    const uint32_t row = first + q * groups + group;
-                    rs[q] = 0;
-                    re[q] = 0;
-                    if (row < ph.row_end) {
-                        rs[q] = poff[row];
-                        re[q] = poff[row + 1];
-                    }
-                    longest = max(longest, re[q] - rs[q]);
-                }
+                for (int q = 0; q < kRowsPerGroup; ++q) longest = max(longest, re[q] - rs[q]);
                 float acc[kRowsPerGroup], comp[kRowsPerGroup];
 #pragma unroll
                 for (int q = 0; q < kRowsPerGroup; ++q) {
@@ -488,6 +519,17 @@ __global__ void __launch_bounds__(kPrThreads, kRowCtasPerSm) pr_rows_kernel(
                     my_diff += to_fixed(d);
                     my_dangle += to_fixed(dg);
                 }
+            }
+            if (!kPrefetchRows && nb < sched.total_blocks) {
+                npi = unit_phase(sched, nb);
+                if (sched.phase[npi].kind == kPhaseGroup) unit_rows(sched.phase[npi], nb, lane, poff, nrs, nre);
+            }
+            b = nb;
+            pi = npi;
+#pragma unroll
+            for (int q = 0; q < kRowsPerGroup; ++q) {
+                rs[q] = nrs[q];
+                re[q] = nre[q];
             }
         }
     }
