@@ -250,6 +250,9 @@ __global__ void bfs_queue_to_bitmap_kernel(const uint32_t* __restrict__ queue, u
 }
 
 constexpr uint32_t kBuSolo = 8;  // entries a lane checks alone before its warp takes over the list
+constexpr int kBuBatch = 4;      // loads in flight per lane while it checks its first entries
+// Load the next word's visited bits and list bounds while this word is probed.
+constexpr bool kBuPipelined = false;
 
 __device__ __forceinline__ bool in_frontier(const uint32_t* __restrict__ frontier, uint32_t u) {
     return (__ldg(frontier + (u >> 5)) >> (u & 31)) & 1u;
@@ -271,22 +274,50 @@ __device__ __forceinline__ void bottomup_body(
     const uint64_t words = ceil_div_u64(V, 32);
     const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
     Tally tally;
-    for (uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; w < words; w += warps) {
-        const uint32_t vis = visited[w];
+    // A word's visited bits and its lanes' list bounds, loaded side by side
+    // (the bounds of visited vertices are read too and then ignored, which
+    // keeps the two loads independent). With kBuPipelined the next word's
+    // are loaded while this word's lists are probed; each word is read and
+    // written only by the warp that owns it, so the early read is current.
+    auto fetch = [&](uint64_t word, uint32_t& fvis, uint32_t& fs, uint32_t& fe) {
+        fvis = 0xFFFFFFFFu;
+        fs = 0;
+        fe = 0;
+        if (word < words) {
+            fvis = visited[word];
+            const uint64_t u = word * 32 + lane;
+            if (u < V) {
+                fs = offsets[u];
+                fe = offsets[u + 1];
+            }
+        }
+    };
+    uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    uint32_t cur_vis = 0, cur_s = 0, cur_e = 0;
+    if (kBuPipelined) fetch(w, cur_vis, cur_s, cur_e);
+    for (; w < words; w += warps) {
+        uint32_t next_vis = 0, next_s = 0, next_e = 0;
+        if (kBuPipelined)
+            fetch(w + warps, next_vis, next_s, next_e);
+        else
+            fetch(w, cur_vis, cur_s, cur_e);
+        const uint32_t vis = cur_vis;
         const uint32_t v = static_cast<uint32_t>(w * 32 + lane);
         bool found = false;
-        uint32_t s = 0, e = 0;
-        if (v < V && !((vis >> lane) & 1u)) {
-            s = offsets[v];
-            e = offsets[v + 1];
+        const bool open = v < V && !((vis >> lane) & 1u);
+        const uint32_t s = open ? cur_s : 0, e = open ? cur_e : 0;
+        if (kBuPipelined) {
+            cur_vis = next_vis;
+            cur_s = next_s;
+            cur_e = next_e;
         }
         const uint32_t solo = min(e - s, kBuSolo);
-        for (uint32_t k = 0; k < solo && !found; k += 4) {
-            uint32_t t[4];
+        for (uint32_t k = 0; k < solo && !found; k += kBuBatch) {
+            uint32_t t[kBuBatch];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) t[q] = k + q < solo ? targets[s + k + q] : 0xFFFFFFFFu;
+            for (int q = 0; q < kBuBatch; ++q) t[q] = k + q < solo ? targets[s + k + q] : 0xFFFFFFFFu;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) found = found || (t[q] != 0xFFFFFFFFu && in_frontier(frontier, t[q]));
+            for (int q = 0; q < kBuBatch; ++q) found = found || (t[q] != 0xFFFFFFFFu && in_frontier(frontier, t[q]));
         }
         unsigned pending = __ballot_sync(kFullMask, !found && e - s > kBuSolo);
         while (pending) {
