@@ -20,8 +20,8 @@
 //    of 2^(c-1) lanes per row (1 to 32); a group works on 2 rows in lockstep,
 //    2 steps per trip (a row of class c has fewer than 2g entries, so a third
 //    step would always be masked below class 6), so every lane keeps 4
-//    independent loads in flight (2 CTAs of 768 threads per SM, 40
-//    registers, persistent); consecutive groups read
+//    independent loads in flight within 32 registers (2 CTAs of 1024
+//    threads per SM, persistent); consecutive groups read
 //    consecutive rows (coalesced), and there is no search, staging, barrier or
 //    carry. Rows of 1024 or more entries are split into 1024-entry segments,
 //    one warp each, and their partial sums are added in segment order by the
@@ -52,13 +52,15 @@
 
 namespace gcu {
 
-// Two CTAs of 768 threads per SM: the 24 warps of a CTA hold consecutive
+// Two CTAs of 1024 threads per SM: the 32 warps of a CTA hold consecutive
 // work units, so an SM works on two contiguous windows of rows at a time
-// instead of eight, and their gathers share more L1 lines; 40 registers.
-// Measured per iteration (R-MAT 24 directed / R-MAT 22; same ranks bit for
-// bit): 8 x 256 threads 1.871 / 0.448 ms, 4 x 512 1.833 / 0.434, 2 x 1024
-// (32 registers) 1.778 / 0.437, 2 x 768 1.759 / 0.429.
-constexpr int kPrThreads = 768;
+// instead of eight, and their gathers share more L1 lines; 32 registers, 64
+// warps per SM. Measured per iteration (R-MAT 24 directed / R-MAT 22 /
+// Erdos-Renyi 2^22; same ranks bit for bit): 8 x 256 threads 1.871 / 0.448 /
+// 0.893 ms, 4 x 512 1.833 / 0.434 / -, 2 x 1024 1.778 / 0.437 / 0.882, 2 x 768
+// (40 registers, 48 warps) 1.759 / 0.429 / 0.992: with fewer warps the
+// Erdos-Renyi gathers, none of which hit L1, have fewer loads in flight.
+constexpr int kPrThreads = 1024;
 constexpr int kDegClasses = 33;       // class 0: degree 0; class c: degree in [2^(c-1), 2^c)
 constexpr int kLongClass = 11;        // degree >= 1024
 constexpr uint32_t kSegment = 1024;   // entries per long-row segment (one warp)
@@ -77,8 +79,9 @@ constexpr int kRowCtasPerSm = 2;      // persistent CTAs of the row kernel per S
 // 32K entries ran slower (the carve-out shrinks L1). Off.
 constexpr uint32_t kHubEntries = 0;
 // Load the next group-phase unit's row offsets while working on this one.
-// Measured slower (2 x 768: 1.923 against 1.759 ms per iteration at R-MAT 24
-// directed, 0.480 against 0.429 ms at R-MAT 22): off.
+// It needs 40 registers; measured slower (2 x 768 threads: 1.923 against
+// 1.759 ms per iteration at R-MAT 24 directed, 0.480 against 0.429 ms at
+// R-MAT 22): off.
 constexpr bool kPrefetchRows = false;
 
 enum : uint32_t { kPhaseLong = 0, kPhaseGroup = 1, kPhaseEmpty = 2 };
@@ -360,7 +363,7 @@ __device__ __forceinline__ double group_sum(double v, uint32_t log2g) {
 // degree class, or 32 rows without entries). Every phase's units are spread
 // evenly over the warps, the warps in flight read one contiguous window of
 // the CSR, and no block barrier ties the warps of a CTA together inside the
-// loop. 2 CTAs of 768 threads per SM.
+// loop. 2 CTAs of 1024 threads per SM.
 
 // Phase of work unit b.
 __device__ __forceinline__ uint32_t unit_phase(const PrSchedule& sched, uint32_t b) {
