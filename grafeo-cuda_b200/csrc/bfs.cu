@@ -388,22 +388,28 @@ __global__ void __launch_bounds__(kTdThreads) bfs_topdown_warp_kernel(
     topdown_warp_body(offsets, targets, queue, qsize, dist, visited, next_queue, ctr, next_level);
 }
 
-// One warp: the features of the decision before expanding the frontier the
-// last step produced (its counters, plus the host's totals before that step),
-// written to features_out when given; with a network, the chosen variant goes
-// to ctr->choice for the host to read with the counters.
-// Beamer's direction rule (alpha = 14, beta = 24) over the balanced push and
-// the pull, from the state after a step: the fixed schedule, the fallback of
-// the learned one, and the variant the learned pick has to beat by a margin.
+// Beamer's direction-optimising thresholds (Beamer, Asanovic and Patterson,
+// SC'12): pull when the frontier's edges exceed the unexplored edges / alpha,
+// back to push when the frontier falls below V / beta.
+constexpr int kAlpha = 14;
+constexpr int kBeta = 24;
+
+// Beamer's direction rule over the balanced push and the pull, from the
+// state after a step: the fixed schedule, the fallback of the learned one,
+// and the variant the learned pick has to beat by a margin.
 __host__ __device__ __forceinline__ int bfs_fixed_variant(bool symmetric, bool bottom_up, uint64_t frontier_n,
                                                           uint64_t frontier_m, uint64_t unexplored, uint32_t V) {
-    const double alpha = 14.0, beta = 24.0;
+    const double alpha = kAlpha, beta = kBeta;
     if (!symmetric) return kPushBalanced;
     if (!bottom_up && static_cast<double>(frontier_m) > static_cast<double>(unexplored) / alpha) return kPull;
     if (bottom_up && static_cast<double>(frontier_n) < static_cast<double>(V) / beta) return kPushBalanced;
     return bottom_up ? kPull : kPushBalanced;
 }
 
+// One warp: the features of the decision before expanding the frontier the
+// last step produced (its counters, plus the host's totals before that step),
+// written to features_out when given; with a network, the chosen variant goes
+// to ctr->choice for the host to read with the counters.
 __global__ void bfs_decide_kernel(const __nv_bfloat16* __restrict__ w, BfsCounters* __restrict__ ctr,
                                   DegreeStats stats, unsigned long long prior_unexplored, uint32_t prior_reached,
                                   int32_t frontier_level, int frontier_bitmap, unsigned valid_mask, uint32_t num_nodes,
