@@ -83,6 +83,8 @@ struct BfsWork {
     DeviceBuffer<BfsCounters> counters;
     BfsCounters* host_counters = nullptr;  // pinned
     int symmetric = -1;                    // -1 unknown, 0 no, 1 yes
+    DeviceBuffer<uint32_t> active;         // vertices with edges, ascending (symmetric graphs: the pull walks them)
+    uint32_t n_active = 0;
     // device-driven level loop (built on first use, per schedule network)
     DeviceBuffer<BfsDevState> loop_state;
     DeviceBuffer<uint32_t> loop_scan_sums;
@@ -250,9 +252,9 @@ __global__ void bfs_queue_to_bitmap_kernel(const uint32_t* __restrict__ queue, u
 }
 
 constexpr uint32_t kBuSolo = 8;  // entries a lane checks alone before its warp takes over the list
-constexpr int kBuBatch = 4;      // loads in flight per lane while it checks its first entries
-// Load the next word's visited bits and list bounds while this word is probed.
-constexpr bool kBuPipelined = false;
+// The pull step walks the list of vertices with edges (true) or every word
+// of the visited bitmap (false).
+constexpr bool kBuActiveList = true;
 
 __device__ __forceinline__ bool in_frontier(const uint32_t* __restrict__ frontier, uint32_t u) {
     return (__ldg(frontier + (u >> 5)) >> (u & 31)) & 1u;
@@ -265,6 +267,43 @@ __device__ __forceinline__ bool in_frontier(const uint32_t* __restrict__ frontie
 // 32 consecutive entries per step (coalesced) with a ballot to stop at the
 // first parent, so a long list neither serialises one lane nor stalls the
 // other 31.
+// Whether this lane's vertex (list [s, e); e == s: nothing to probe) has a
+// neighbour in the frontier. Called by all 32 lanes: the lists left after
+// the solo probes are walked by the whole warp.
+__device__ __forceinline__ bool probe_parent(uint32_t s, uint32_t e, const uint32_t* __restrict__ frontier,
+                                             const uint32_t* __restrict__ targets) {
+    const unsigned lane = lane_id();
+    bool found = false;
+    const uint32_t solo = min(e - s, kBuSolo);
+    for (uint32_t k = 0; k < solo && !found; k += 4) {
+        uint32_t t[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) t[q] = k + q < solo ? targets[s + k + q] : 0xFFFFFFFFu;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) found = found || (t[q] != 0xFFFFFFFFu && in_frontier(frontier, t[q]));
+    }
+    unsigned pending = __ballot_sync(kFullMask, !found && e - s > kBuSolo);
+    while (pending) {
+        const int p = __ffs(pending) - 1;
+        pending &= pending - 1;
+        const uint64_t ps = static_cast<uint64_t>(__shfl_sync(kFullMask, s, p)) + kBuSolo;
+        const uint64_t pe = __shfl_sync(kFullMask, e, p);
+        bool hit = false;
+        for (uint64_t base = ps; base < pe; base += 32) {
+            const uint64_t j = base + lane;
+            const bool h = j < pe && in_frontier(frontier, targets[j]);
+            if (__ballot_sync(kFullMask, h)) {
+                hit = true;
+                break;
+            }
+        }
+        if (static_cast<int>(lane) == p) found = hit;
+    }
+    return found;
+}
+
+// Word form: warp w handles the 32 vertices of bitmap word w (it owns that
+// word of `visited` and writes the word of `next_frontier`, found or not).
 __device__ __forceinline__ void bottomup_body(
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t V,
     const uint32_t* __restrict__ frontier, uint32_t* __restrict__ next_frontier, uint32_t* __restrict__ visited,
@@ -274,68 +313,19 @@ __device__ __forceinline__ void bottomup_body(
     const uint64_t words = ceil_div_u64(V, 32);
     const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
     Tally tally;
-    // A word's visited bits and its lanes' list bounds, loaded side by side
-    // (the bounds of visited vertices are read too and then ignored, which
-    // keeps the two loads independent). With kBuPipelined the next word's
-    // are loaded while this word's lists are probed; each word is read and
-    // written only by the warp that owns it, so the early read is current.
-    auto fetch = [&](uint64_t word, uint32_t& fvis, uint32_t& fs, uint32_t& fe) {
-        fvis = 0xFFFFFFFFu;
-        fs = 0;
-        fe = 0;
-        if (word < words) {
-            fvis = visited[word];
-            const uint64_t u = word * 32 + lane;
-            if (u < V) {
-                fs = offsets[u];
-                fe = offsets[u + 1];
-            }
-        }
-    };
-    uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    uint32_t cur_vis = 0, cur_s = 0, cur_e = 0;
-    if (kBuPipelined) fetch(w, cur_vis, cur_s, cur_e);
-    for (; w < words; w += warps) {
-        uint32_t next_vis = 0, next_s = 0, next_e = 0;
-        if (kBuPipelined)
-            fetch(w + warps, next_vis, next_s, next_e);
-        else
-            fetch(w, cur_vis, cur_s, cur_e);
-        const uint32_t vis = cur_vis;
+    for (uint64_t w = (static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; w < words; w += warps) {
+        // The word's visited bits and its lanes' list bounds, loaded side by
+        // side (the bounds of visited vertices are read too, then ignored).
+        const uint32_t vis = visited[w];
         const uint32_t v = static_cast<uint32_t>(w * 32 + lane);
-        bool found = false;
+        uint32_t s = 0, e = 0;
+        if (v < V) {
+            s = offsets[v];
+            e = offsets[v + 1];
+        }
         const bool open = v < V && !((vis >> lane) & 1u);
-        const uint32_t s = open ? cur_s : 0, e = open ? cur_e : 0;
-        if (kBuPipelined) {
-            cur_vis = next_vis;
-            cur_s = next_s;
-            cur_e = next_e;
-        }
-        const uint32_t solo = min(e - s, kBuSolo);
-        for (uint32_t k = 0; k < solo && !found; k += kBuBatch) {
-            uint32_t t[kBuBatch];
-#pragma unroll
-            for (int q = 0; q < kBuBatch; ++q) t[q] = k + q < solo ? targets[s + k + q] : 0xFFFFFFFFu;
-#pragma unroll
-            for (int q = 0; q < kBuBatch; ++q) found = found || (t[q] != 0xFFFFFFFFu && in_frontier(frontier, t[q]));
-        }
-        unsigned pending = __ballot_sync(kFullMask, !found && e - s > kBuSolo);
-        while (pending) {
-            const int p = __ffs(pending) - 1;
-            pending &= pending - 1;
-            const uint64_t ps = static_cast<uint64_t>(__shfl_sync(kFullMask, s, p)) + kBuSolo;
-            const uint64_t pe = __shfl_sync(kFullMask, e, p);
-            bool hit = false;
-            for (uint64_t base = ps; base < pe; base += 32) {
-                const uint64_t j = base + lane;
-                const bool h = j < pe && in_frontier(frontier, targets[j]);
-                if (__ballot_sync(kFullMask, h)) {
-                    hit = true;
-                    break;
-                }
-            }
-            if (static_cast<int>(lane) == p) found = hit;
-        }
+        if (!open) e = s;
+        const bool found = probe_parent(s, e, frontier, targets);
         const unsigned mask = __ballot_sync(kFullMask, found);
         if (lane == 0) {
             next_frontier[w] = mask;
@@ -346,12 +336,54 @@ __device__ __forceinline__ void bottomup_body(
     flush_tally(tally, ctr);
 }
 
+// List form: the warps stride over the graph's vertices with edges (`active`,
+// ascending), 32 at a time, so no lane sits on an isolated vertex (43 % of
+// R-MAT 22's). A word of the bitmaps can span two warps' batches, so found
+// vertices set their bits with atomicOr; the caller clears next_frontier.
+__device__ __forceinline__ void bottomup_list_body(
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets,
+    const uint32_t* __restrict__ active, uint32_t n_active, const uint32_t* __restrict__ frontier,
+    uint32_t* __restrict__ next_frontier, uint32_t* visited, int32_t* __restrict__ dist,
+    uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr, int32_t next_level) {
+    const unsigned lane = lane_id();
+    const uint64_t warps = (static_cast<uint64_t>(gridDim.x) * blockDim.x) >> 5;
+    Tally tally;
+    for (uint64_t base = ((static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * 32; base < n_active;
+         base += warps * 32) {
+        const uint64_t i = base + lane;
+        uint32_t v = 0, s = 0, e = 0;
+        bool open = false;
+        if (i < n_active) {
+            v = active[i];
+            // Only this lane sets its vertex's bit, so a word another warp is
+            // updating still shows this bit as it is.
+            const uint32_t vis = visited[v >> 5];
+            s = offsets[v];
+            e = offsets[v + 1];
+            open = !((vis >> (v & 31)) & 1u);
+        }
+        if (!open) e = s;
+        const bool found = probe_parent(s, e, frontier, targets);
+        if (found) {
+            const uint32_t bit = 1u << (v & 31);
+            atomicOr(next_frontier + (v >> 5), bit);
+            atomicOr(visited + (v >> 5), bit);
+        }
+        record_discovery(found, v, offsets, dist, next_level, next_queue, ctr, tally);
+    }
+    flush_tally(tally, ctr);
+}
+
 __global__ void __launch_bounds__(kBuThreads) bfs_bottomup_kernel(
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t V,
-    const uint32_t* __restrict__ frontier, uint32_t* __restrict__ next_frontier, uint32_t* __restrict__ visited,
-    int32_t* __restrict__ dist, uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr,
-    int32_t next_level) {
-    bottomup_body(offsets, targets, V, frontier, next_frontier, visited, dist, next_queue, ctr, next_level);
+    const uint32_t* __restrict__ active, uint32_t n_active, const uint32_t* __restrict__ frontier,
+    uint32_t* __restrict__ next_frontier, uint32_t* __restrict__ visited, int32_t* __restrict__ dist,
+    uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr, int32_t next_level) {
+    if (kBuActiveList)
+        bottomup_list_body(offsets, targets, active, n_active, frontier, next_frontier, visited, dist, next_queue, ctr,
+                           next_level);
+    else
+        bottomup_body(offsets, targets, V, frontier, next_frontier, visited, dist, next_queue, ctr, next_level);
 }
 
 // Top-down, one warp per frontier vertex (no degree scan: one launch, for
@@ -595,15 +627,43 @@ __global__ void bfs_queue_to_bitmap_loop_kernel(const uint32_t* queue0, const ui
 }
 
 __global__ void __launch_bounds__(kBuThreads) bfs_bottomup_loop_kernel(
-    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t V, uint32_t* bitmap0,
-    uint32_t* bitmap1, uint32_t* __restrict__ visited, int32_t* __restrict__ dist, uint32_t* queue0,
-    uint32_t* queue1, BfsCounters* __restrict__ ctr, const BfsDevState* __restrict__ st) {
+    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t V,
+    const uint32_t* __restrict__ active, uint32_t n_active, uint32_t* bitmap0, uint32_t* bitmap1,
+    uint32_t* __restrict__ visited, int32_t* __restrict__ dist, uint32_t* queue0, uint32_t* queue1,
+    BfsCounters* __restrict__ ctr, const BfsDevState* __restrict__ st) {
     const uint32_t cur = st->cur;
-    bottomup_body(offsets, targets, V, cur ? bitmap1 : bitmap0, cur ? bitmap0 : bitmap1, visited, dist,
-                  cur ? queue0 : queue1, ctr, st->level + 1);
+    if (kBuActiveList)
+        bottomup_list_body(offsets, targets, active, n_active, cur ? bitmap1 : bitmap0, cur ? bitmap0 : bitmap1,
+                           visited, dist, cur ? queue0 : queue1, ctr, st->level + 1);
+    else
+        bottomup_body(offsets, targets, V, cur ? bitmap1 : bitmap0, cur ? bitmap0 : bitmap1, visited, dist,
+                      cur ? queue0 : queue1, ctr, st->level + 1);
+}
+
+// The list form of the pull sets only found bits: clear the bitmap it fills.
+__global__ void bfs_next_bitmap_clear_loop_kernel(uint32_t* bitmap0, uint32_t* bitmap1, uint64_t words,
+                                                  const BfsDevState* __restrict__ st) {
+    uint32_t* bitmap = st->cur ? bitmap0 : bitmap1;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < words;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        bitmap[i] = 0;
 }
 
 // ---------------------------------------------------------------- host
+
+// The vertices with at least one entry, ascending (flags, scan, scatter).
+__global__ void bfs_has_edges_kernel(const uint32_t* __restrict__ offsets, uint32_t V, uint32_t* __restrict__ flags) {
+    for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
+         v += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        flags[v] = offsets[v + 1] > offsets[v] ? 1u : 0u;
+}
+
+__global__ void bfs_active_scatter_kernel(const uint32_t* __restrict__ offsets, uint32_t V,
+                                          const uint32_t* __restrict__ pos, uint32_t* __restrict__ active) {
+    for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < V;
+         v += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        if (offsets[v + 1] > offsets[v]) active[pos[v]] = static_cast<uint32_t>(v);
+}
 
 static Error ensure_work(GraphImpl& g) {
     if (g.bfs_work) return ok();
@@ -624,6 +684,21 @@ static Error ensure_work(GraphImpl& g) {
     bool sym = false;
     GCU_TRY(graph_symmetry(g, &sym));
     w->symmetric = sym ? 1 : 0;
+    if (sym && kBuActiveList && V > 0) {
+        // degree_scan is free until the first balanced push: flags, then positions.
+        const unsigned grid = static_cast<unsigned>(
+            std::min<uint64_t>(ceil_div_u64(V, 256), static_cast<uint64_t>(dev.sm_count) * 16));
+        GCU_LAUNCH(dev, "bfs_has_edges", bfs_has_edges_kernel, grid, 256, 0, g.offsets.ptr, static_cast<uint32_t>(V),
+                   w->degree_scan.ptr);
+        GCU_TRY(exclusive_scan_u32(dev, w->degree_scan.ptr, w->degree_scan.ptr, V));
+        uint32_t n = 0;
+        GCU_CUDA(cudaMemcpyAsync(&n, w->degree_scan.ptr + V, sizeof(n), cudaMemcpyDeviceToHost, dev.stream), "copy");
+        GCU_TRY(dev.sync());
+        GCU_TRY(w->active.allocate(dev, std::max<uint32_t>(n, 1)));
+        GCU_LAUNCH(dev, "bfs_active_scatter", bfs_active_scatter_kernel, grid, 256, 0, g.offsets.ptr,
+                   static_cast<uint32_t>(V), w->degree_scan.ptr, w->active.ptr);
+        w->n_active = n;
+    }
     g.bfs_work = w.release();
     return ok();
 }
@@ -666,10 +741,14 @@ Error launch_step(GraphImpl& g, BfsWork& w, int variant, const BfsState& st) {
             GCU_LAUNCH(dev, "bfs_queue_to_bitmap", bfs_queue_to_bitmap_kernel, blocks, 256, 0, w.queue[cur].ptr,
                        st.frontier_q, w.bitmap[cur].ptr);
         }
-        unsigned blocks = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(words * 32, kBuThreads), grid_cap));
+        const uint64_t lanes = kBuActiveList ? w.n_active : words * 32;
+        if (kBuActiveList)
+            GCU_CUDA(cudaMemsetAsync(w.bitmap[nxt].ptr, 0, sizeof(uint32_t) * words, dev.stream), "memset");
+        unsigned blocks = static_cast<unsigned>(
+            std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(lanes, kBuThreads), grid_cap)));
         GCU_LAUNCH(dev, "bfs_bottomup", bfs_bottomup_kernel, blocks, kBuThreads, 0, g.offsets.ptr, g.targets.ptr, V,
-                   w.bitmap[cur].ptr, w.bitmap[nxt].ptr, w.visited.ptr, w.dist.ptr, w.queue[nxt].ptr, w.counters.ptr,
-                   st.level + 1);
+                   w.active.ptr, w.n_active, w.bitmap[cur].ptr, w.bitmap[nxt].ptr, w.visited.ptr, w.dist.ptr,
+                   w.queue[nxt].ptr, w.counters.ptr, st.level + 1);
     } else if (variant == kPushWarp) {
         unsigned blocks = static_cast<unsigned>(
             std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(st.frontier_q, kTdThreads / 32), grid_cap)));
@@ -771,8 +850,8 @@ Error build_loop_graph(GraphImpl& g, BfsWork& w) {
     const uint32_t* n_ptr = &st->frontier_q;
     const unsigned cap = static_cast<unsigned>(dev.sm_count) * 16;
     const unsigned vgrid = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(V, 256), cap)));
-    const unsigned bu_grid =
-        static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(words * 32, kBuThreads), cap)));
+    const unsigned bu_grid = static_cast<unsigned>(std::max<uint64_t>(
+        1, std::min<uint64_t>(ceil_div_u64(kBuActiveList ? w.n_active : words * 32, kBuThreads), cap)));
     const unsigned wgrid =
         static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(V, kTdThreads / 32), cap)));
     const unsigned td_grid = static_cast<unsigned>(dev.sm_count) * 8;
@@ -867,9 +946,12 @@ Error build_loop_graph(GraphImpl& g, BfsWork& w) {
                    w.bitmap[1].ptr, words, st);
         GCU_LAUNCH(dev, "bfs_queue_to_bitmap", bfs_queue_to_bitmap_loop_kernel, vgrid, 256, 0, w.queue[0].ptr,
                    w.queue[1].ptr, w.bitmap[0].ptr, w.bitmap[1].ptr, st);
+        if (kBuActiveList)
+            GCU_LAUNCH(dev, "bfs_next_bitmap_clear", bfs_next_bitmap_clear_loop_kernel, vgrid, 256, 0,
+                       w.bitmap[0].ptr, w.bitmap[1].ptr, words, st);
         GCU_LAUNCH(dev, "bfs_bottomup", bfs_bottomup_loop_kernel, bu_grid, kBuThreads, 0, g.offsets.ptr,
-                   g.targets.ptr, V, w.bitmap[0].ptr, w.bitmap[1].ptr, w.visited.ptr, w.dist.ptr, w.queue[0].ptr,
-                   w.queue[1].ptr, w.counters.ptr, st);
+                   g.targets.ptr, V, w.active.ptr, w.n_active, w.bitmap[0].ptr, w.bitmap[1].ptr, w.visited.ptr,
+                   w.dist.ptr, w.queue[0].ptr, w.queue[1].ptr, w.counters.ptr, st);
         return ok();
     }));
     cudaGraphExec_t exec = nullptr;
