@@ -378,12 +378,17 @@ __device__ __forceinline__ void bottomup_list_body(
     flush_tally(tally, ctr);
 }
 
+// One instantiation per pull form (kList: walk `active`; else every bitmap
+// word), so that each keeps its own body's register count: the word form
+// needs 32 registers, a kernel holding both bodies 38, which costs a quarter
+// of the resident warps of whichever form runs.
+template <bool kList>
 __global__ void __launch_bounds__(kBuThreads) bfs_bottomup_kernel(
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t V,
     const uint32_t* __restrict__ active, uint32_t n_active, const uint32_t* __restrict__ frontier,
     uint32_t* __restrict__ next_frontier, uint32_t* __restrict__ visited, int32_t* __restrict__ dist,
     uint32_t* __restrict__ next_queue, BfsCounters* __restrict__ ctr, int32_t next_level) {
-    if (active)
+    if (kList)
         bottomup_list_body(offsets, targets, active, n_active, frontier, next_frontier, visited, dist, next_queue, ctr,
                            next_level);
     else
@@ -630,13 +635,14 @@ __global__ void bfs_queue_to_bitmap_loop_kernel(const uint32_t* queue0, const ui
     }
 }
 
+template <bool kList>  // one instantiation per pull form, as bfs_bottomup_kernel
 __global__ void __launch_bounds__(kBuThreads) bfs_bottomup_loop_kernel(
     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ targets, uint32_t V,
     const uint32_t* __restrict__ active, uint32_t n_active, uint32_t* bitmap0, uint32_t* bitmap1,
     uint32_t* __restrict__ visited, int32_t* __restrict__ dist, uint32_t* queue0, uint32_t* queue1,
     BfsCounters* __restrict__ ctr, const BfsDevState* __restrict__ st) {
     const uint32_t cur = st->cur;
-    if (active)
+    if (kList)
         bottomup_list_body(offsets, targets, active, n_active, cur ? bitmap1 : bitmap0, cur ? bitmap0 : bitmap1,
                            visited, dist, cur ? queue0 : queue1, ctr, st->level + 1);
     else
@@ -753,7 +759,8 @@ Error launch_step(GraphImpl& g, BfsWork& w, int variant, const BfsState& st) {
             GCU_CUDA(cudaMemsetAsync(w.bitmap[nxt].ptr, 0, sizeof(uint32_t) * words, dev.stream), "memset");
         unsigned blocks = static_cast<unsigned>(
             std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(lanes, kBuThreads), grid_cap)));
-        GCU_LAUNCH(dev, "bfs_bottomup", bfs_bottomup_kernel, blocks, kBuThreads, 0, g.offsets.ptr, g.targets.ptr, V,
+        const auto bottomup = w.pull_list ? bfs_bottomup_kernel<true> : bfs_bottomup_kernel<false>;
+        GCU_LAUNCH(dev, "bfs_bottomup", bottomup, blocks, kBuThreads, 0, g.offsets.ptr, g.targets.ptr, V,
                    w.pull_list ? w.active.ptr : nullptr, w.n_active, w.bitmap[cur].ptr, w.bitmap[nxt].ptr, w.visited.ptr, w.dist.ptr,
                    w.queue[nxt].ptr, w.counters.ptr, st.level + 1);
     } else if (variant == kPushWarp) {
@@ -956,7 +963,8 @@ Error build_loop_graph(GraphImpl& g, BfsWork& w) {
         if (w.pull_list)
             GCU_LAUNCH(dev, "bfs_next_bitmap_clear", bfs_next_bitmap_clear_loop_kernel, vgrid, 256, 0,
                        w.bitmap[0].ptr, w.bitmap[1].ptr, words, st);
-        GCU_LAUNCH(dev, "bfs_bottomup", bfs_bottomup_loop_kernel, bu_grid, kBuThreads, 0, g.offsets.ptr,
+        const auto bottomup = w.pull_list ? bfs_bottomup_loop_kernel<true> : bfs_bottomup_loop_kernel<false>;
+        GCU_LAUNCH(dev, "bfs_bottomup", bottomup, bu_grid, kBuThreads, 0, g.offsets.ptr,
                    g.targets.ptr, V, w.pull_list ? w.active.ptr : nullptr, w.n_active, w.bitmap[0].ptr, w.bitmap[1].ptr, w.visited.ptr,
                    w.dist.ptr, w.queue[0].ptr, w.queue[1].ptr, w.counters.ptr, st);
         return ok();
