@@ -89,6 +89,10 @@ def parse_args():
                     help="instead of the headline: BFS from 16 random sources on R-MAT 22, Erdos-Renyi 2^22 and "
                          "R-MAT 24, device time per search with the level loop on the device and on the host, "
                          "against the sum of its kernels' CUDA-event times, per kernel; one JSON document")
+    ap.add_argument("--pr-ceiling", action="store_true",
+                    help="instead of the headline: PageRank's row kernel per iteration against the gather probe "
+                         "(its plan's target stream and contribution gathers alone) on R-MAT 22, Erdos-Renyi 2^22 "
+                         "and the R-MAT 24 directed copy; one JSON document")
     return ap.parse_args()
 
 
@@ -754,10 +758,62 @@ def run_bfs_breakdown() -> dict:
     return out
 
 
+def run_pr_ceiling() -> dict:
+    """PageRank's row kernel against the floor of a pull SpMV on its own plan:
+    per graph, pr_rows' device time per iteration (per-kernel CUDA events, a
+    fixed iteration count) and the gather probe's device time per pass (the
+    plan's relabelled targets streamed and each contribution gathered, nothing
+    else, same grid and CTA shape; median of 3 x 20 passes)."""
+    import grafeo_cuda as G
+
+    dev = G.GpuDevice(0)
+    out = {"pr_ceiling": "pr_rows ms per iteration against the gather probe's ms per pass on the same plan",
+           "device": dev.name}
+    for name in ("rmat22", "er22", "rmat24"):
+        if name == "rmat24":
+            g0 = G.GpuGraph.generate_rmat(dev, 24, EDGE_FACTOR, *RMAT_ABC, seed=5)
+            csr = g0.to_csr()
+            del g0
+            off, tgt, _ = directed_dangling_copy(csr.offsets, csr.targets, 0.03, 5)
+            del csr
+            g = G.GpuGraph.from_csr(off, tgt, dev)
+            directed, iters = True, 38
+            run = lambda: g.pagerank_directed(0.85, iters, 0.0, copy_result=False)  # noqa: E731
+        else:
+            if name == "rmat22":
+                g = G.GpuGraph.generate_rmat(dev, 22, EDGE_FACTOR, *RMAT_ABC, seed=2)
+            else:
+                g = G.GpuGraph.generate_erdos_renyi(dev, 1 << 22, 16 << 22, seed=3)
+            directed, iters = False, 50
+            run = lambda: g.pagerank_array(0.85, iters, 0.0, copy_result=False)  # noqa: E731
+        V, E = g.num_nodes, g.num_edges
+        run()
+        dev.set_kernel_timing(True)
+        dev.reset_stats()
+        r = run()
+        launches, rows_ms = dev.kernel_stats()["pr_rows"]
+        dev.set_kernel_timing(False)
+        per_it = rows_ms / r["iterations"]
+        probe = float(np.median([g.pagerank_gather_probe(directed, 20) for _ in range(3)]))
+        out[name] = {
+            "vertices": V, "in_csr_entries": E, "iterations": r["iterations"], "pr_rows_launches": launches,
+            "pr_rows_ms_per_iteration": round(per_it, 4),
+            "gather_probe_ms_per_pass": round(probe, 4),
+            "pr_rows_over_probe": round(per_it / probe, 3) if probe else None,
+            "pr_rows_gbs_algorithmic": round(pr_bytes(V, E) / (per_it / 1e3) / 1e9, 1),
+            "probe_gbs_of_4E": round(4 * E / (probe / 1e3) / 1e9, 1) if probe else None,
+        }
+        del g
+    return out
+
+
 def main():
     args = parse_args()
     if args.bfs_breakdown:
         print(json.dumps(run_bfs_breakdown()), flush=True)
+        return
+    if args.pr_ceiling:
+        print(json.dumps(run_pr_ceiling()), flush=True)
         return
     d = Dist()
     try:

@@ -273,6 +273,11 @@ Error transpose_csr(DeviceImpl& dev, const uint32_t* offsets, const uint32_t* ta
 Error pagerank_ex(GraphImpl& g, bool directed, const float* tele, float damping, uint32_t max_iterations,
                   float tolerance, float* host_ranks, uint32_t* iterations, bool* converged);
 
+// Times `passes` launches of the gather probe (the plan's target stream and
+// contribution gathers alone) over the plan of pagerank_ex(directed); builds
+// the plan if needed. *ms_per_pass = device time per launch.
+Error pagerank_gather_probe(GraphImpl& g, bool directed, uint32_t passes, double* ms_per_pass);
+
 void destroy_pagerank_plan(PageRankPlan* p);
 void destroy_bfs_work(BfsWork* w);
 void destroy_kt_cache(KtCache* c);

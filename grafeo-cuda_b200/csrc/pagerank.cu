@@ -772,6 +772,80 @@ static Error ensure_plan(GraphImpl& g, bool directed, PageRankPlan** plan) {
     return ok();
 }
 
+// Gather probe: the relabelled targets streamed coalesced and contrib[t]
+// gathered, with nothing else (no row offsets, no row structure, no
+// epilogue). Same grid, CTA shape and load pattern (8 targets, then 8
+// gathers, in flight per lane) as the long-row segments of pr_rows, over the
+// same plan, so its time per pass is the floor of a pull SpMV on this layout.
+// Each warp folds its sums into one float atomic so that nothing is dropped.
+__global__ void __launch_bounds__(kPrThreads, kRowCtasPerSm) pr_gather_probe_kernel(
+    const uint32_t* __restrict__ ptgt, uint32_t E, const float* __restrict__ contrib, float* __restrict__ sink) {
+    const uint32_t total_warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned lane = lane_id();
+    float acc = 0.f;
+    for (uint64_t base = static_cast<uint64_t>(warp) * kSegment; base < E;
+         base += static_cast<uint64_t>(total_warps) * kSegment) {
+        const uint64_t end = min_u64(base + kSegment, E);
+        uint64_t j = base + lane;
+        for (; j + 7 * 32 < end; j += 8 * 32) {
+            uint32_t t[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) t[q] = ld_stream(ptgt + j + q * 32);
+            float c[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) c[q] = __ldg(contrib + t[q]);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) acc += c[q];
+        }
+        for (; j < end; j += 32) acc += __ldg(contrib + ld_stream(ptgt + j));
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) atomicAdd(sink, acc);
+}
+
+Error pagerank_gather_probe(GraphImpl& g, bool directed, uint32_t passes, double* ms_per_pass) {
+    *ms_per_pass = 0.0;
+    const uint32_t V = g.num_nodes, E = g.num_edges;
+    if (V == 0 || E == 0 || passes == 0) return ok();
+    DeviceImpl& dev = *g.dev;
+    PageRankPlan* plan = nullptr;
+    GCU_TRY(ensure_plan(g, directed, &plan));
+    PageRankPlan& p = *plan;
+    const uint64_t cap = static_cast<uint64_t>(dev.sm_count) * 16;
+    const unsigned vgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
+    GCU_LAUNCH(dev, "pr_init", pr_init_kernel, vgrid, 256, 0, p.poff.ptr, directed ? p.outdeg.ptr : nullptr, V,
+               1.0f / static_cast<float>(V), p.ranks.ptr, p.contrib.ptr);
+    DeviceBuffer<float> sink;
+    GCU_TRY(sink.allocate(dev, 1));
+    GCU_CUDA(cudaMemsetAsync(sink.ptr, 0, sizeof(float), dev.stream), "memset");
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    GCU_CUDA(cudaEventCreate(&ev[0]), "cudaEventCreate");
+    cudaError_t c = cudaEventCreate(&ev[1]);
+    Error err = ok();
+    if (c != cudaSuccess) err = kernel_error(std::string("cudaEventCreate: ") + cudaGetErrorString(c));
+    if (err.ok()) {
+        err = [&]() -> Error {
+            GCU_LAUNCH(dev, "pr_gather_probe", pr_gather_probe_kernel, p.row_ctas, kPrThreads, 0, p.ptgt.ptr, E,
+                       p.contrib.ptr, sink.ptr);  // warm-up
+            GCU_CUDA(cudaEventRecord(ev[0], dev.stream), "cudaEventRecord");
+            for (uint32_t i = 0; i < passes; ++i)
+                GCU_LAUNCH(dev, "pr_gather_probe", pr_gather_probe_kernel, p.row_ctas, kPrThreads, 0, p.ptgt.ptr, E,
+                           p.contrib.ptr, sink.ptr);
+            GCU_CUDA(cudaEventRecord(ev[1], dev.stream), "cudaEventRecord");
+            GCU_CUDA(cudaEventSynchronize(ev[1]), "cudaEventSynchronize");
+            float ms = 0.f;
+            GCU_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]), "cudaEventElapsedTime");
+            *ms_per_pass = static_cast<double>(ms) / passes;
+            return ok();
+        }();
+    }
+    for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    GCU_TRY(err);
+    return dev.sync();
+}
+
 Error pagerank_ex(GraphImpl& g, bool directed, const float* tele_host, float damping, uint32_t max_iterations,
                   float tolerance, float* host_ranks, uint32_t* iterations, bool* converged) {
     const uint32_t V = g.num_nodes;

@@ -605,6 +605,16 @@ GCU_API gcu_status gcu_pagerank_directed(gcu_graph* g, float damping, uint32_t m
     return succeed();
 }
 
+GCU_API gcu_status gcu_pagerank_gather_probe(gcu_graph* g, int directed, uint32_t passes, double* ms_per_pass) {
+    if (!g || !ms_per_pass) return fail(kernel_error("graph or result pointer is NULL"));
+    GraphImpl& gi = *g->impl;
+    std::lock_guard<std::mutex> lock(gi.mu);
+    Error e = gi.dev->activate();
+    if (e.ok()) e = pagerank_gather_probe(gi, directed != 0, passes, ms_per_pass);
+    if (!e.ok()) return fail(e);
+    return succeed();
+}
+
 GCU_API gcu_status gcu_personalized_pagerank(gcu_graph* g, const uint32_t* seeds, size_t n_seeds, int directed,
                                              float damping, uint32_t max_iterations, float tolerance, float* ranks,
                                              uint32_t* iterations, int* converged, double* seconds) {

@@ -466,6 +466,15 @@ class GpuGraph:
             copy_result,
         )
 
+    def pagerank_gather_probe(self, directed: bool = False, passes: int = 20) -> float:
+        """Device ms per launch of the gather probe over this graph's PageRank
+        plan (the target stream and contribution gathers alone): the floor of
+        a pull SpMV on that layout. A diagnostic; builds the plan if needed."""
+        passes = self._check_u32(passes, "passes")
+        ms = C.c_double()
+        check(lib.gcu_pagerank_gather_probe(self._h, 1 if directed else 0, passes, C.byref(ms)))
+        return ms.value
+
     def personalized_pagerank(self, seeds, damping: float = 0.85, max_iterations: int = 100,
                               tolerance: float = 1e-6, directed: bool = False, copy_result: bool = True) -> dict:
         """PageRank whose teleport and dangling mass go to `seeds` uniformly."""

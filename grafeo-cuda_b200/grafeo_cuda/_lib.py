@@ -142,6 +142,10 @@ SIGNATURES = {
             C.POINTER(C.c_double),
         ],
     ),
+    "gcu_pagerank_gather_probe": (
+        C.c_int,
+        [C.c_void_p, C.c_int, C.c_uint32, C.POINTER(C.c_double)],
+    ),
     "gcu_k_truss": (
         C.c_int,
         [C.c_void_p, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_uint32), C.POINTER(C.c_double)],

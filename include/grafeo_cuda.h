@@ -249,6 +249,15 @@ GCU_API gcu_status gcu_personalized_pagerank(gcu_graph* g, const uint32_t* seeds
                                              float damping, uint32_t max_iterations, float tolerance, float* ranks,
                                              uint32_t* iterations, int* converged, double* seconds);
 
+/* Diagnostic, no reference counterpart: the floor of a pull SpMV on the
+ * PageRank plan. Times `passes` launches (after one warm-up) of a kernel that
+ * streams the plan's relabelled in-CSR targets and gathers the contribution
+ * of each, with nothing else (no row offsets or row structure, no rank
+ * update), on the grid and CTA shape of the PageRank row kernel.
+ * *ms_per_pass = device time per launch. directed as in
+ * gcu_personalized_pagerank; builds the plan if needed. */
+GCU_API gcu_status gcu_pagerank_gather_probe(gcu_graph* g, int directed, uint32_t passes, double* ms_per_pass);
+
 typedef struct gcu_edge_list gcu_edge_list; /* Vec<(u32, u32)>, host memory */
 
 /* k_truss::k_truss(graph, k) (k_truss.rs:42-161). Edges (u, v) with u < v in

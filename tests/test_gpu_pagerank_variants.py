@@ -106,3 +106,18 @@ def test_personalized_pagerank_argument_errors(device):
     with pytest.raises(GrafeoCudaError) as e:
         g.personalized_pagerank([2])
     assert e.value.status == G.ERR_KERNEL and "out of range" in str(e.value)
+
+
+def test_gather_probe_times_the_plan_and_leaves_results_alone(device):
+    """The diagnostic gather probe runs over the PageRank plan (built on
+    demand, directed or not), returns a positive device time, and later
+    PageRank calls give the same ranks bit for bit."""
+    g = G.GpuGraph.generate_rmat(device, 14, 16, 0.57, 0.19, 0.19, seed=1)
+    before = g.pagerank_array(0.85, 30, 0.0)["ranks"]
+    ms = g.pagerank_gather_probe(False, 5)
+    assert np.isfinite(ms) and ms > 0
+    assert np.array_equal(g.pagerank_array(0.85, 30, 0.0)["ranks"], before)
+    directed_before = g.pagerank_directed(0.85, 30, 0.0)["ranks"]
+    assert g.pagerank_gather_probe(True, 3) > 0
+    assert np.array_equal(g.pagerank_directed(0.85, 30, 0.0)["ranks"], directed_before)
+    assert g.pagerank_gather_probe(False, 0) == 0.0
