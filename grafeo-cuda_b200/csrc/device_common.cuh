@@ -65,6 +65,12 @@ __device__ __forceinline__ uint32_t ld_stream(const uint32_t* p) {
     return v;
 }
 
+__device__ __forceinline__ uint2 ld_stream2(const uint2* p) {
+    uint2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v2.u32 {%0,%1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+    return v;
+}
+
 __device__ __forceinline__ uint4 ld_stream4(const uint4* p) {
     uint4 v;
     asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0,%1,%2,%3}, [%4];"

@@ -84,6 +84,24 @@ constexpr uint32_t kHubEntries = 0;
 // R-MAT 22): off.
 constexpr bool kPrefetchRows = false;
 
+// Rows of 1 to 1023 entries, read as a stream of chunks: kChunk consecutive
+// entries of the relabelled CSR per warp (rows packed back to back, a row
+// that crosses a chunk boundary split between the chunks), 8 consecutive
+// entries per lane, loaded as two 128-bit target loads and one 64-bit load of
+// their row deltas (row minus the chunk's first row: a chunk holds at most
+// kChunk rows, each with an entry, so a byte holds it). A lane sums its runs
+// of equal rows, a segmented scan over the warp joins the runs that cross
+// lanes, and the lane where a row ends finishes it; the parts of a row that
+// crosses chunks are added, in chunk order, by the finishing kernel. Every
+// lane keeps 8 gathers in flight with no row offsets in the chain, against
+// 1 to 2 entries per lane and row in the lane-group form (kChunkRows = false:
+// rows of class c served by groups of 2^(c-1) lanes).
+constexpr bool kChunkRows = true;
+constexpr uint32_t kChunk = 256;
+constexpr int kChunkThreads = 512;
+constexpr int kChunkCtasPerSm = 2;
+constexpr uint32_t kNoRow = 0xFFFFFFFFu;
+
 enum : uint32_t { kPhaseLong = 0, kPhaseGroup = 1, kPhaseEmpty = 2 };
 
 struct PrPhase {
@@ -131,6 +149,14 @@ struct PageRankPlan {
     DeviceBuffer<unsigned long long> fin_partials; // 2 per block of the finishing kernel
     DeviceBuffer<PrState> state;
     PrState* host_state = nullptr;     // pinned
+    // Chunked rows (kChunkRows): entries [chunk_lo, chunk_hi) of the relabelled
+    // CSR, chunk c covering entries chunk_origin + kChunk c .. + kChunk - 1.
+    uint32_t chunk_origin = 0, chunk_lo = 0, chunk_hi = 0;
+    uint32_t n_chunks = 0, n_split = 0, chunk_ctas = 0;
+    DeviceBuffer<uint32_t> chunk_row;   // first row of each chunk
+    DeviceBuffer<uint8_t> chunk_delta;  // per entry: its row minus its chunk's first row
+    DeviceBuffer<uint4> split_rows;     // (row, first chunk, last chunk, 0) of the rows that cross chunks
+    DeviceBuffer<double> chunk_part;    // per chunk: the part of its first row (begun before it), of its last row (going on)
 };
 
 void destroy_pagerank_plan(PageRankPlan* p) {
@@ -239,12 +265,16 @@ constexpr int kFillThreads = 256;
 constexpr int kFillItems = 4;
 constexpr int kFillTile = kFillThreads * kFillItems;
 
+// With `delta`, entries in [lo, hi) also get their chunk row delta.
 __global__ void __launch_bounds__(kFillThreads) pr_perm_fill_kernel(const uint32_t* __restrict__ offsets,
                                                                     const uint32_t* __restrict__ targets,
                                                                     const uint32_t* __restrict__ perm,
                                                                     const uint32_t* __restrict__ inv,
                                                                     const uint32_t* __restrict__ poff, uint32_t V,
-                                                                    uint32_t E, uint32_t* __restrict__ ptgt) {
+                                                                    uint32_t E, uint32_t* __restrict__ ptgt,
+                                                                    const uint32_t* __restrict__ chunk_row,
+                                                                    uint32_t origin, uint32_t lo, uint32_t hi,
+                                                                    uint8_t* __restrict__ delta) {
     __shared__ uint32_t s_start[kFillTile];
     __shared__ uint32_t s_meta[2];
     for (uint64_t e0 = static_cast<uint64_t>(blockIdx.x) * kFillTile; e0 < E;
@@ -259,8 +289,38 @@ __global__ void __launch_bounds__(kFillThreads) pr_perm_fill_kernel(const uint32
             const uint32_t r = tile_row(poff, V, s_start, staged, r0, nrows, static_cast<uint32_t>(k));
             const uint32_t src = offsets[perm[r]] + static_cast<uint32_t>(k - poff[r]);
             ptgt[k] = inv[ld_stream(targets + src)];
+            if (delta && k >= lo && k < hi) {
+                const uint32_t rel = static_cast<uint32_t>(k) - origin;
+                delta[rel] = static_cast<uint8_t>(r - chunk_row[rel / kChunk]);
+            }
         }
         __syncthreads();  // the staged starts are rewritten for the next tile
+    }
+}
+
+// Chunk c's first row is the row holding its first entry (chunk 0: the first
+// chunked row, which may begin a few entries into it); a row of the chunked
+// range [r0, r1) is split when its entries fall in more than one chunk.
+__global__ void pr_chunk_rows_kernel(const uint32_t* __restrict__ poff, uint32_t r0, uint32_t r1, uint32_t origin,
+                                     uint32_t* __restrict__ chunk_row, uint32_t* __restrict__ split_flag) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < r1 - r0;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t r = r0 + static_cast<uint32_t>(i);
+        const uint32_t s = poff[r] - origin, e = poff[r + 1] - origin;  // e > s: every chunked row has entries
+        const uint32_t c_first = s / kChunk, c_last = (e - 1) / kChunk;
+        for (uint32_t c = r == r0 ? 0 : (s + kChunk - 1) / kChunk; c <= c_last; ++c) chunk_row[c] = r;
+        split_flag[i] = c_first != c_last ? 1u : 0u;
+    }
+}
+
+__global__ void pr_split_rows_kernel(const uint32_t* __restrict__ poff, uint32_t r0, uint32_t n, uint32_t origin,
+                                     const uint32_t* __restrict__ split_pos, uint4* __restrict__ split_rows) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        if (split_pos[i + 1] == split_pos[i]) continue;
+        const uint32_t r = r0 + static_cast<uint32_t>(i);
+        split_rows[split_pos[i]] =
+            make_uint4(r, (poff[r] - origin) / kChunk, (poff[r + 1] - 1 - origin) / kChunk, 0u);
     }
 }
 
@@ -557,15 +617,137 @@ __global__ void __launch_bounds__(kPrThreads, kRowCtasPerSm) pr_rows_kernel(
     }
 }
 
+// One warp per chunk of kChunk entries (chunks dealt round-robin to the warps
+// of a persistent grid), 8 consecutive entries per lane. Row sums are FP64
+// (the contributions are FP32). A run of equal rows inside a lane that is
+// neither its first nor its last is a whole row; the first and last runs are
+// joined across lanes by a segmented scan, and the lane where a run ends
+// finishes its row, except for the parts of rows that cross chunks:
+// chunk_part[2c] takes the part of chunk c's first row when that row began
+// in an earlier chunk, chunk_part[2c + 1] the part of its last row when that
+// row goes on into the next chunk (the whole chunk when one row covers it).
+__global__ void __launch_bounds__(kChunkThreads, kChunkCtasPerSm) pr_chunks_kernel(
+    const uint32_t* __restrict__ poff, const uint32_t* __restrict__ ptgt, const uint8_t* __restrict__ delta,
+    const uint32_t* __restrict__ chunk_row, uint32_t origin, uint32_t lo, uint32_t hi, uint32_t n_chunks,
+    const float* __restrict__ rank_in, const float* __restrict__ contrib_in, float* __restrict__ rank_out,
+    float* __restrict__ contrib_out, const uint32_t* __restrict__ outdeg, const float* __restrict__ tele, uint32_t V,
+    double base, double damp, const PrState* __restrict__ state, double* __restrict__ chunk_part,
+    unsigned long long* __restrict__ partials) {
+    if (state->done) return;
+    constexpr int kWarps = kChunkThreads / 32;
+    __shared__ double s_mass[2];
+    __shared__ unsigned long long s_sum[2 * kWarps];
+    if (threadIdx.x == 0) {
+        s_mass[0] = state->dangling;
+        s_mass[1] = state->dangling / static_cast<double>(V);
+    }
+    __syncthreads();
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    const uint32_t total_warps = (gridDim.x * blockDim.x) >> 5;
+    unsigned long long my_diff = 0, my_dangle = 0;
+    auto finish = [&](uint32_t r, double sum) {
+        double d = 0.0, dg = 0.0;
+        pr_finish_row(r, sum, poff[r + 1] - poff[r], rank_in, rank_out, contrib_out, outdeg, tele, base, damp,
+                      s_mass[1], s_mass[0], d, dg);
+        my_diff += to_fixed(d);
+        my_dangle += to_fixed(dg);
+    };
+    for (uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_chunks; c += total_warps) {
+        const uint32_t e0 = origin + c * kChunk;   // chunk start; entries [e0, e0 + kChunk)
+        const uint32_t eb = e0 + 8 * lane;         // this lane's first entry (32-byte aligned)
+        const uint32_t rbase = __ldg(chunk_row + c);
+        const uint4 ta = ld_stream4(reinterpret_cast<const uint4*>(ptgt + eb));
+        const uint4 tb = ld_stream4(reinterpret_cast<const uint4*>(ptgt + eb + 4));
+        const uint2 dl = ld_stream2(reinterpret_cast<const uint2*>(delta + (eb - origin)));
+        const bool first_split = __ldg(poff + rbase) < e0;  // the first row began in an earlier chunk
+        const uint32_t t[8] = {ta.x, ta.y, ta.z, ta.w, tb.x, tb.y, tb.z, tb.w};
+        uint32_t row[8];
+        float val[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const uint32_t e = eb + i;
+            const bool ok = e >= lo && e < hi;
+            row[i] = ok ? rbase + (((i < 4 ? dl.x : dl.y) >> (8 * (i & 3))) & 0xFFu) : kNoRow;
+            val[i] = ok ? __ldg(contrib_in + t[i]) : 0.f;
+        }
+        const uint32_t rlast = __shfl_sync(kFullMask, row[7], 31);
+        // Only the last chunk has slots past `hi`, and its last row ends inside it.
+        const bool last_split = rlast != kNoRow && __ldg(poff + rlast + 1) > e0 + kChunk;
+        double head = 0.0, acc = 0.0;
+        bool multi = false;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            acc += static_cast<double>(val[i]);
+            if (i < 7 && row[i + 1] != row[i]) {
+                if (!multi) {
+                    head = acc;
+                    multi = true;
+                } else {
+                    finish(row[i], acc);  // a whole row inside this lane (never kNoRow: those runs lead or trail)
+                }
+                acc = 0.0;
+            }
+        }
+        // Segmented inclusive scan of the lanes' last runs: a lane continues the
+        // run of the lane before when it holds one row only and that row is the
+        // previous lane's last.
+        const uint32_t rf = row[0], rl = row[7];
+        const uint32_t prev_last = __shfl_up_sync(kFullMask, rl, 1);
+        const uint32_t next_first = __shfl_down_sync(kFullMask, rf, 1);
+        const bool carry_in = lane > 0 && prev_last == rf;
+        bool head_flag = multi || !carry_in;
+        double S = acc;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double su = __shfl_up_sync(kFullMask, S, d);
+            const bool fu = __shfl_up_sync(kFullMask, head_flag, d);
+            if (lane >= static_cast<unsigned>(d)) {
+                if (!head_flag) S += su;
+                head_flag = head_flag || fu;
+            }
+        }
+        const double carry = __shfl_up_sync(kFullMask, S, 1);
+        if (multi && rf != kNoRow) {  // the first run ends in this lane
+            const double total = head + (carry_in ? carry : 0.0);
+            if (rf == rbase && first_split) chunk_part[2 * static_cast<uint64_t>(c)] = total;
+            else finish(rf, total);
+        }
+        const bool continues = lane < 31 && next_first == rl;
+        if (!continues && rl != kNoRow) {  // the last run ends at this lane's end
+            if (lane == 31 && last_split) chunk_part[2 * static_cast<uint64_t>(c) + 1] = S;
+            else if (rl == rbase && first_split) chunk_part[2 * static_cast<uint64_t>(c)] = S;
+            else finish(rl, S);
+        }
+    }
+    my_diff = warp_sum(my_diff);
+    my_dangle = warp_sum(my_dangle);
+    if (lane == 0) {
+        s_sum[2 * warp] = my_diff;
+        s_sum[2 * warp + 1] = my_dangle;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long diff = 0, dangle = 0;
+        for (int w = 0; w < kWarps; ++w) {
+            diff += s_sum[2 * w];
+            dangle += s_sum[2 * w + 1];
+        }
+        partials[2 * blockIdx.x] = diff;
+        partials[2 * blockIdx.x + 1] = dangle;
+    }
+}
+
 // Finishes the long rows from their segment partials (in segment order) and
-// folds a fixed slice of kFinSlice row-kernel block partials per block; then
+// the chunked rows that cross chunks from their chunk parts (in chunk order),
+// and folds a fixed slice of kFinSlice row-kernel block partials per block; then
 // the last block reduces the per-block results in a fixed order and advances
 // the state.
 constexpr uint32_t kFinSlice = 2048;
 
 __global__ void __launch_bounds__(256) pr_finish_kernel(
     const uint32_t* __restrict__ poff, uint32_t long_rows, const uint32_t* __restrict__ unit_begin,
-    const double* __restrict__ seg_partial, const float* __restrict__ rank_in, float* __restrict__ rank_out,
+    const double* __restrict__ seg_partial, const uint4* __restrict__ split_rows, uint32_t n_split,
+    const double* __restrict__ chunk_part, const float* __restrict__ rank_in, float* __restrict__ rank_out,
     float* __restrict__ contrib_out, const uint32_t* __restrict__ outdeg, const float* __restrict__ tele, uint32_t V,
     double base, double damp, PrState* __restrict__ state,
     double tolerance, const unsigned long long* __restrict__ row_partials, uint32_t row_blocks,
@@ -582,6 +764,17 @@ __global__ void __launch_bounds__(256) pr_finish_kernel(
         for (uint32_t u = unit_begin[i]; u < unit_begin[i + 1]; ++u) sum += seg_partial[u];
         pr_finish_row(i, sum, poff[i + 1] - poff[i], rank_in, rank_out, contrib_out, outdeg, tele, base, damp,
                       spread, dangling, rd, rg);
+        d = to_fixed(rd);
+        g = to_fixed(rg);
+    } else if (i - long_rows < n_split) {
+        // A chunked row that crosses chunks: its part in its first chunk (that
+        // chunk's last row), every chunk it covers whole, its part in its last.
+        const uint4 sr = split_rows[i - long_rows];
+        double sum = chunk_part[2 * static_cast<uint64_t>(sr.y) + 1], rd = 0.0, rg = 0.0;
+        for (uint32_t c = sr.y + 1; c < sr.z; ++c) sum += chunk_part[2 * static_cast<uint64_t>(c) + 1];
+        sum += chunk_part[2 * static_cast<uint64_t>(sr.z)];
+        pr_finish_row(sr.x, sum, poff[sr.x + 1] - poff[sr.x], rank_in, rank_out, contrib_out, outdeg, tele, base,
+                      damp, spread, dangling, rd, rg);
         d = to_fixed(rd);
         g = to_fixed(rg);
     }
@@ -651,22 +844,6 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
     GCU_CUDA(cudaMemsetAsync(starts.ptr + kDegClasses + 1, 0, sizeof(uint32_t), dev.stream), "memset");
     GCU_LAUNCH(dev, "pr_class_starts", pr_class_starts_kernel, 1, 64, 0, cpos.ptr, nblk, starts.ptr);
 
-    // 2. Relabelled CSR (and out-degrees when they differ from the row lengths).
-    GCU_TRY(p.poff.allocate(dev, static_cast<uint64_t>(V) + 1));
-    GCU_TRY(p.ptgt.allocate(dev, E));
-    GCU_LAUNCH(dev, "pr_perm_degree", pr_perm_degree_kernel, vgrid, 256, 0, pull_offsets, p.perm.ptr, V, p.poff.ptr);
-    GCU_TRY(exclusive_scan_u32(dev, p.poff.ptr, p.poff.ptr, V));
-    if (E > 0) {
-        const unsigned fill_grid =
-            static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(E, kFillTile), cap)));
-        GCU_LAUNCH(dev, "pr_perm_fill", pr_perm_fill_kernel, fill_grid, kFillThreads, 0, pull_offsets, pull_targets,
-                   p.perm.ptr, p.inv.ptr, p.poff.ptr, V, E, p.ptgt.ptr);
-    }
-    if (out_offsets) {
-        GCU_TRY(p.outdeg.allocate(dev, V));
-        GCU_LAUNCH(dev, "pr_outdeg", pr_outdeg_kernel, vgrid, 256, 0, out_offsets, p.perm.ptr, V, p.outdeg.ptr,
-                   starts.ptr + kDegClasses + 1);
-    }
     uint32_t cls[kDegClasses + 2];
     GCU_CUDA(cudaMemcpyAsync(cls, starts.ptr, sizeof(cls), cudaMemcpyDeviceToHost, dev.stream), "copy");
     GCU_TRY(dev.sync());
@@ -679,7 +856,71 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
     }
     p.long_rows = begin[kLongClass - 1];  // classes >= kLongClass occupy [0, begin[kLongClass - 1])
     p.empty_rows = end[0] - begin[0];
-    p.dangling_rows = out_offsets ? cls[kDegClasses + 1] : p.empty_rows;
+
+    // 2. Relabelled CSR (and out-degrees when they differ from the row lengths).
+    GCU_TRY(p.poff.allocate(dev, static_cast<uint64_t>(V) + 1));
+    GCU_LAUNCH(dev, "pr_perm_degree", pr_perm_degree_kernel, vgrid, 256, 0, pull_offsets, p.perm.ptr, V, p.poff.ptr);
+    GCU_TRY(exclusive_scan_u32(dev, p.poff.ptr, p.poff.ptr, V));
+    // Chunked rows: [long_rows, begin[0]), entries [chunk_lo, chunk_hi). The
+    // chunk kernel indexes entries in 32 bits up to kChunk past E, so graphs
+    // within 2 kChunk of 2^32 entries keep the lane-group form.
+    const uint32_t short_rows = begin[0] - p.long_rows;
+    if (kChunkRows && short_rows > 0 && E <= 0xFFFFFFFFu - 2 * kChunk) {
+        uint32_t bounds[2];
+        GCU_CUDA(cudaMemcpyAsync(&bounds[0], p.poff.ptr + p.long_rows, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 dev.stream),
+                 "copy");
+        GCU_CUDA(cudaMemcpyAsync(&bounds[1], p.poff.ptr + begin[0], sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 dev.stream),
+                 "copy");
+        GCU_TRY(dev.sync());
+        p.chunk_lo = bounds[0];
+        p.chunk_hi = bounds[1];
+        p.chunk_origin = p.chunk_lo & ~7u;  // 32-byte aligned target loads
+        p.n_chunks = static_cast<uint32_t>(ceil_div_u64(p.chunk_hi - p.chunk_origin, kChunk));
+        GCU_TRY(p.chunk_row.allocate(dev, p.n_chunks));
+        GCU_TRY(p.chunk_delta.allocate(dev, static_cast<uint64_t>(p.n_chunks) * kChunk));
+        GCU_TRY(p.chunk_part.allocate(dev, 2 * static_cast<uint64_t>(p.n_chunks)));
+        GCU_CUDA(cudaMemsetAsync(p.chunk_delta.ptr, 0, static_cast<size_t>(p.n_chunks) * kChunk, dev.stream),
+                 "memset");
+        DeviceBuffer<uint32_t> split_pos;
+        GCU_TRY(split_pos.allocate(dev, static_cast<uint64_t>(short_rows) + 1));
+        const unsigned sgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(short_rows, 256), cap));
+        GCU_LAUNCH(dev, "pr_chunk_rows", pr_chunk_rows_kernel, sgrid, 256, 0, p.poff.ptr, p.long_rows, begin[0],
+                   p.chunk_origin, p.chunk_row.ptr, split_pos.ptr);
+        GCU_TRY(exclusive_scan_u32(dev, split_pos.ptr, split_pos.ptr, short_rows));
+        GCU_CUDA(cudaMemcpyAsync(&p.n_split, split_pos.ptr + short_rows, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 dev.stream),
+                 "copy");
+        GCU_TRY(dev.sync());
+        GCU_TRY(p.split_rows.allocate(dev, std::max<uint32_t>(p.n_split, 1)));
+        GCU_LAUNCH(dev, "pr_split_rows", pr_split_rows_kernel, sgrid, 256, 0, p.poff.ptr, p.long_rows, short_rows,
+                   p.chunk_origin, split_pos.ptr, p.split_rows.ptr);
+    }
+    // The last chunk's loads run up to kChunk entries past E: padding of valid ids.
+    const uint64_t tgt_pad = p.n_chunks ? kChunk : 0;
+    GCU_TRY(p.ptgt.allocate(dev, static_cast<uint64_t>(E) + tgt_pad));
+    if (tgt_pad) GCU_CUDA(cudaMemsetAsync(p.ptgt.ptr + E, 0, sizeof(uint32_t) * tgt_pad, dev.stream), "memset");
+    if (E > 0) {
+        const unsigned fill_grid =
+            static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>(ceil_div_u64(E, kFillTile), cap)));
+        GCU_LAUNCH(dev, "pr_perm_fill", pr_perm_fill_kernel, fill_grid, kFillThreads, 0, pull_offsets, pull_targets,
+                   p.perm.ptr, p.inv.ptr, p.poff.ptr, V, E, p.ptgt.ptr, p.chunk_row.ptr, p.chunk_origin, p.chunk_lo,
+                   p.chunk_hi, p.n_chunks ? p.chunk_delta.ptr : nullptr);
+    }
+    if (out_offsets) {
+        GCU_TRY(p.outdeg.allocate(dev, V));
+        GCU_LAUNCH(dev, "pr_outdeg", pr_outdeg_kernel, vgrid, 256, 0, out_offsets, p.perm.ptr, V, p.outdeg.ptr,
+                   starts.ptr + kDegClasses + 1);
+        uint32_t dangling = 0;
+        GCU_CUDA(cudaMemcpyAsync(&dangling, starts.ptr + kDegClasses + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 dev.stream),
+                 "copy");
+        GCU_TRY(dev.sync());
+        p.dangling_rows = dangling;
+    } else {
+        p.dangling_rows = p.empty_rows;
+    }
 
     // 3. Long-row segments.
     std::vector<uint32_t> long_off(p.long_rows + 1, 0);
@@ -708,7 +949,8 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
                              cudaMemcpyHostToDevice, dev.stream),
              "copy");
 
-    // 4. Block schedule: long segments, then classes kLongClass-1 .. 1, then empty rows.
+    // 4. Block schedule: long segments, then (unless chunked) classes
+    // kLongClass-1 .. 1, then empty rows.
     PrSchedule& s = p.sched;
     s.nphases = 0;
     uint32_t blocks = 0;
@@ -724,7 +966,7 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
         blocks += nb;
     };
     add(kPhaseLong, 0, p.long_rows, 0, 0, static_cast<uint32_t>(units.size()));
-    for (int c = kLongClass - 1; c >= 1; --c) {
+    for (int c = kLongClass - 1; c >= 1 && p.n_chunks == 0; --c) {
         // Class c (degrees [2^(c-1), 2^c)): 2^(c-1) lanes per row up to a warp.
         const uint32_t rows = end[c] - begin[c];
         const uint32_t log2g = std::min<uint32_t>(static_cast<uint32_t>(c - 1), 5);
@@ -740,13 +982,18 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
         GCU_CUDA(cudaFuncSetAttribute(pr_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       static_cast<int>(kHubEntries * sizeof(float))),
                  "cudaFuncSetAttribute");
-    p.fin_blocks = static_cast<uint32_t>(
-        std::max<uint64_t>({1, ceil_div_u64(p.long_rows, 256), ceil_div_u64(p.row_ctas, kFinSlice)}));
+    p.chunk_ctas = p.n_chunks == 0 ? 0
+                                   : std::max<uint32_t>(1, std::min<uint32_t>(
+                                                               ceil_div_u64(p.n_chunks, kChunkThreads / 32),
+                                                               static_cast<uint32_t>(dev.sm_count) * kChunkCtasPerSm));
+    p.fin_blocks = static_cast<uint32_t>(std::max<uint64_t>(
+        {1, ceil_div_u64(static_cast<uint64_t>(p.long_rows) + p.n_split, 256),
+         ceil_div_u64(static_cast<uint64_t>(p.row_ctas) + p.chunk_ctas, kFinSlice)}));
 
     GCU_TRY(p.ranks.allocate(dev, 2 * static_cast<uint64_t>(V)));
     GCU_TRY(p.contrib.allocate(dev, 2 * static_cast<uint64_t>(V)));
     GCU_TRY(p.ranks_out.allocate(dev, V));
-    GCU_TRY(p.row_partials.allocate(dev, 2 * static_cast<uint64_t>(p.row_ctas)));
+    GCU_TRY(p.row_partials.allocate(dev, 2 * (static_cast<uint64_t>(p.row_ctas) + p.chunk_ctas)));
     GCU_TRY(p.fin_partials.allocate(dev, 2 * static_cast<uint64_t>(p.fin_blocks)));
     GCU_TRY(p.state.allocate(dev, 1));
     GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p.host_state), sizeof(PrState)), "cudaMallocHost");
@@ -776,7 +1023,8 @@ static Error ensure_plan(GraphImpl& g, bool directed, PageRankPlan** plan) {
 // gathered, with nothing else (no row offsets, no row structure, no
 // epilogue). Same grid, CTA shape and load pattern (8 targets, then 8
 // gathers, in flight per lane) as the long-row segments of pr_rows, over the
-// same plan, so its time per pass is the floor of a pull SpMV on this layout.
+// same plan, so its time per pass is the floor of a pull SpMV on this layout
+// (the grid is the row kernel's full persistent grid, 2 CTAs per SM).
 // Each warp folds its sums into one float atomic so that nothing is dropped.
 __global__ void __launch_bounds__(kPrThreads, kRowCtasPerSm) pr_gather_probe_kernel(
     const uint32_t* __restrict__ ptgt, uint32_t E, const float* __restrict__ contrib, float* __restrict__ sink) {
@@ -816,6 +1064,7 @@ Error pagerank_gather_probe(GraphImpl& g, bool directed, uint32_t passes, double
     const unsigned vgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(V, 256), cap));
     GCU_LAUNCH(dev, "pr_init", pr_init_kernel, vgrid, 256, 0, p.poff.ptr, directed ? p.outdeg.ptr : nullptr, V,
                1.0f / static_cast<float>(V), p.ranks.ptr, p.contrib.ptr);
+    const unsigned grid = static_cast<unsigned>(dev.sm_count) * kRowCtasPerSm;  // the row kernel's full grid
     DeviceBuffer<float> sink;
     GCU_TRY(sink.allocate(dev, 1));
     GCU_CUDA(cudaMemsetAsync(sink.ptr, 0, sizeof(float), dev.stream), "memset");
@@ -826,11 +1075,11 @@ Error pagerank_gather_probe(GraphImpl& g, bool directed, uint32_t passes, double
     if (c != cudaSuccess) err = kernel_error(std::string("cudaEventCreate: ") + cudaGetErrorString(c));
     if (err.ok()) {
         err = [&]() -> Error {
-            GCU_LAUNCH(dev, "pr_gather_probe", pr_gather_probe_kernel, p.row_ctas, kPrThreads, 0, p.ptgt.ptr, E,
+            GCU_LAUNCH(dev, "pr_gather_probe", pr_gather_probe_kernel, grid, kPrThreads, 0, p.ptgt.ptr, E,
                        p.contrib.ptr, sink.ptr);  // warm-up
             GCU_CUDA(cudaEventRecord(ev[0], dev.stream), "cudaEventRecord");
             for (uint32_t i = 0; i < passes; ++i)
-                GCU_LAUNCH(dev, "pr_gather_probe", pr_gather_probe_kernel, p.row_ctas, kPrThreads, 0, p.ptgt.ptr, E,
+                GCU_LAUNCH(dev, "pr_gather_probe", pr_gather_probe_kernel, grid, kPrThreads, 0, p.ptgt.ptr, E,
                            p.contrib.ptr, sink.ptr);
             GCU_CUDA(cudaEventRecord(ev[1], dev.stream), "cudaEventRecord");
             GCU_CUDA(cudaEventSynchronize(ev[1]), "cudaEventSynchronize");
@@ -906,9 +1155,16 @@ Error pagerank_ex(GraphImpl& g, bool directed, const float* tele_host, float dam
                            p.poff.ptr, p.ptgt.ptr,
                            ranks[in], contrib[in], ranks[out], contrib[out], outdeg, d_tele, V, base, damp,
                            p.state.ptr, p.sched, p.units.ptr, p.seg_partial.ptr, p.row_partials.ptr);
+                if (p.n_chunks > 0)
+                    GCU_LAUNCH(dev, "pr_chunks", pr_chunks_kernel, p.chunk_ctas, kChunkThreads, 0, p.poff.ptr,
+                               p.ptgt.ptr, p.chunk_delta.ptr, p.chunk_row.ptr, p.chunk_origin, p.chunk_lo,
+                               p.chunk_hi, p.n_chunks, ranks[in], contrib[in], ranks[out], contrib[out], outdeg,
+                               d_tele, V, base, damp, p.state.ptr, p.chunk_part.ptr,
+                               p.row_partials.ptr + 2 * static_cast<uint64_t>(p.row_ctas));
                 GCU_LAUNCH(dev, "pr_finish", pr_finish_kernel, p.fin_blocks, 256, 0, p.poff.ptr, p.long_rows,
-                           p.unit_begin.ptr, p.seg_partial.ptr, ranks[in], ranks[out], contrib[out], outdeg, d_tele,
-                           V, base, damp, p.state.ptr, tol, p.row_partials.ptr, p.row_ctas, p.fin_partials.ptr);
+                           p.unit_begin.ptr, p.seg_partial.ptr, p.split_rows.ptr, p.n_split, p.chunk_part.ptr,
+                           ranks[in], ranks[out], contrib[out], outdeg, d_tele, V, base, damp, p.state.ptr, tol,
+                           p.row_partials.ptr, p.row_ctas + p.chunk_ctas, p.fin_partials.ptr);
                 return ok();
             }();
         }
