@@ -16,23 +16,25 @@
 //    hit L1/L2 lines that are already hot. The relabelled CSR keeps every
 //    list in its original order, so each row's summation order is the
 //    original one.
-//  * Rows of one class have similar length, so each class gets a fixed group
-//    of 2^(c-1) lanes per row (1 to 32); a group works on 2 rows in lockstep,
-//    2 steps per trip (a row of class c has fewer than 2g entries, so a third
-//    step would always be masked below class 6), so every lane keeps 4
-//    independent loads in flight within 32 registers (2 CTAs of 1024
-//    threads per SM, persistent); consecutive groups read
-//    consecutive rows (coalesced), and there is no search, staging, barrier or
-//    carry. Rows of 1024 or more entries are split into 1024-entry segments,
-//    one warp each, and their partial sums are added in segment order by the
-//    finishing kernel.
-//  * Work units (a long-row segment, one warp's rows of a class, or 32 rows
-//    without entries) are dealt round-robin to the warps of the persistent
-//    grid: every class is spread evenly, the warps in flight read one
-//    contiguous window of the CSR, and no block barrier ties the warps of a
-//    CTA together.
-//  * Row sums: FP32 Kahan sums per lane, FP64 across lanes (shuffle tree) and
-//    across segments. Epilogue per row v: r'[v] = (1-d)/N + d (sum +
+//  * Rows of 1024 or more entries (the relabelling puts them first) are split
+//    into 1024-entry segments, one warp each, 8 loads in flight per lane, and
+//    their partial sums are added in segment order by the finishing kernel.
+//  * Rows of 1 to 1023 entries (pr_chunks_kernel) are read as a stream of
+//    256-entry chunks, one warp per chunk and 8 consecutive entries per lane
+//    (two 128-bit target loads and one 64-bit load of the entries' row deltas,
+//    a byte each), so every lane keeps 8 gathers in flight whatever the row
+//    lengths; runs of equal rows are summed per lane, joined across lanes by a
+//    warp segmented scan, and finished by the lane where they end, and the
+//    rows that cross chunks are finished from their per-chunk parts, in chunk
+//    order, by the finishing kernel. The lane-group form it replaced (a group
+//    of 2^(c-1) lanes per row of class c, 1 to 2 entries per lane and row)
+//    stays behind kChunkRows = false.
+//  * Work units (a long-row segment, a chunk, or 32 rows without entries)
+//    are dealt round-robin to the warps of persistent grids: the warps in
+//    flight read one contiguous window of the CSR, and no block barrier ties
+//    the warps of a CTA together.
+//  * Row sums: FP32 Kahan sums per lane and FP64 across lanes and segments for
+//    the long rows, FP64 for the chunked rows. Epilogue per row v: r'[v] = (1-d)/N + d (sum +
 //    dangling/N); |r' - r| and the dangling mass of r' are summed as 64-bit
 //    fixed-point integers (2^-62 units) in registers per lane, then per warp
 //    and per CTA, and reduced by the last block of the finishing kernel (no

@@ -72,6 +72,90 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint6
     }
 }
 
+// The same stable scatter with the tile staged in shared memory. Each warp
+// owns a contiguous slice of kSliceKeys keys (kKeysPerLane per lane, loaded
+// coalesced and kept in registers). Pass 1 counts the slice's digits with
+// warp matches; one barrier later every digit has its start inside the tile
+// and every warp its offset inside each digit; pass 2 ranks the keys again in
+// the same order and stores them in shared memory in digit order (index order
+// inside a digit: stable); the block then writes the tile out run by run,
+// consecutive threads to consecutive addresses of a digit's output range.
+constexpr bool kStagedScatter = true;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSliceKeys = kSortTile / kSortWarps;
+constexpr int kKeysPerLane = kSliceKeys / 32;
+
+__global__ void __launch_bounds__(kSortThreads, 3) radix_scatter_staged_kernel(const uint64_t* __restrict__ in,
+                                                                            uint64_t* __restrict__ out, uint64_t n,
+                                                                            uint32_t shift, uint32_t ntiles,
+                                                                            const uint32_t* __restrict__ bases) {
+    __shared__ uint64_t s_keys[kSortTile];
+    __shared__ uint32_t s_woff[kSortWarps][kRadix];  // per warp: digit counts, then running offsets
+    __shared__ uint32_t s_start[kRadix];             // digit start inside the tile
+    __shared__ uint32_t s_base[kRadix];              // digit's output base for this tile
+    __shared__ uint32_t s_wtot[kSortWarps];
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1;
+    for (int w = 0; w < kSortWarps; ++w) s_woff[w][threadIdx.x] = 0;
+    s_base[threadIdx.x] = bases[static_cast<uint64_t>(threadIdx.x) * ntiles + blockIdx.x];
+    const uint64_t tile0 = static_cast<uint64_t>(blockIdx.x) * kSortTile;
+    const uint64_t slice = tile0 + static_cast<uint64_t>(warp) * kSliceKeys;
+    uint64_t key[kKeysPerLane];
+#pragma unroll
+    for (int q = 0; q < kKeysPerLane; ++q) {
+        const uint64_t i = slice + static_cast<uint64_t>(q) * 32 + lane;
+        key[q] = i < n ? in[i] : 0;
+    }
+    // Digit of key q (kRadix: past the end of the input).
+    auto digit = [&](int q) -> uint32_t {
+        return slice + static_cast<uint64_t>(q) * 32 + lane < n ? static_cast<uint32_t>((key[q] >> shift) & 0xFF)
+                                                                 : static_cast<uint32_t>(kRadix);
+    };
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kKeysPerLane; ++q) {
+        const uint32_t d = digit(q);
+        const unsigned same = __match_any_sync(kFullMask, d);
+        if (d < kRadix && lane == static_cast<unsigned>(__ffs(same) - 1)) s_woff[warp][d] += __popc(same);
+        __syncwarp();
+    }
+    __syncthreads();
+    {
+        // Thread d: the warps' exclusive offsets inside digit d, then the
+        // digits' exclusive starts inside the tile (block-wide scan).
+        const uint32_t d = threadIdx.x;
+        uint32_t tot = 0;
+        for (int w = 0; w < kSortWarps; ++w) {
+            const uint32_t c = s_woff[w][d];
+            s_woff[w][d] = tot;
+            tot += c;
+        }
+        const uint32_t inc = warp_inclusive_scan(tot);
+        if (lane == 31) s_wtot[warp] = inc;
+        __syncthreads();
+        uint32_t before = 0;
+        for (unsigned w = 0; w < warp; ++w) before += s_wtot[w];
+        s_start[d] = before + inc - tot;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kKeysPerLane; ++q) {
+        const uint32_t d = digit(q);
+        const unsigned same = __match_any_sync(kFullMask, d);
+        if (d < kRadix) s_keys[s_start[d] + s_woff[warp][d] + __popc(same & below)] = key[q];
+        __syncwarp();
+        if (d < kRadix && lane == static_cast<unsigned>(__ffs(same) - 1)) s_woff[warp][d] += __popc(same);
+        __syncwarp();
+    }
+    __syncthreads();
+    const uint32_t valid = static_cast<uint32_t>(min_u64(kSortTile, n - tile0));
+    for (uint32_t j = threadIdx.x; j < valid; j += kSortThreads) {
+        const uint64_t k = s_keys[j];
+        const uint32_t d = static_cast<uint32_t>((k >> shift) & 0xFF);
+        out[s_base[d] + (j - s_start[d])] = k;
+    }
+}
+
 Error radix_sort_u64(DeviceImpl& dev, uint64_t* keys, uint64_t* tmp, uint64_t n, uint32_t low_bit, uint32_t high_bit,
                      uint64_t** sorted) {
     *sorted = keys;
@@ -87,8 +171,12 @@ Error radix_sort_u64(DeviceImpl& dev, uint64_t* keys, uint64_t* tmp, uint64_t n,
     for (uint32_t shift = low_bit; shift < high_bit; shift += 8) {
         GCU_LAUNCH(dev, "radix_hist", radix_hist_kernel, ntiles, kSortThreads, 0, src, n, shift, ntiles, hist.ptr);
         GCU_TRY(exclusive_scan_u32(dev, hist.ptr, bases.ptr, static_cast<uint64_t>(ntiles) * kRadix));
-        GCU_LAUNCH(dev, "radix_scatter", radix_scatter_kernel, ntiles, kSortThreads, 0, src, dst, n, shift, ntiles,
-                   bases.ptr);
+        if (kStagedScatter)
+            GCU_LAUNCH(dev, "radix_scatter", radix_scatter_staged_kernel, ntiles, kSortThreads, 0, src, dst, n, shift,
+                       ntiles, bases.ptr);
+        else
+            GCU_LAUNCH(dev, "radix_scatter", radix_scatter_kernel, ntiles, kSortThreads, 0, src, dst, n, shift, ntiles,
+                       bases.ptr);
         std::swap(src, dst);
     }
     *sorted = src;
