@@ -85,6 +85,20 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSliceKeys = kSortTile / kSortWarps;
 constexpr int kKeysPerLane = kSliceKeys / 32;
 
+// Lanes of the warp holding the same digit (kRadix: a lane with no key), from
+// one ballot per digit bit (kMatchBallots) or one match instruction.
+constexpr bool kMatchBallots = true;
+__device__ __forceinline__ unsigned same_digit_lanes(uint32_t d) {
+    if (!kMatchBallots) return __match_any_sync(kFullMask, d);
+    unsigned m = __ballot_sync(kFullMask, d == kRadix) ^ (d == kRadix ? 0u : kFullMask);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const unsigned bits = __ballot_sync(kFullMask, (d >> b) & 1u);
+        m &= ((d >> b) & 1u) ? bits : ~bits;
+    }
+    return m;
+}
+
 __global__ void __launch_bounds__(kSortThreads, 3) radix_scatter_staged_kernel(const uint64_t* __restrict__ in,
                                                                             uint64_t* __restrict__ out, uint64_t n,
                                                                             uint32_t shift, uint32_t ntiles,
@@ -115,7 +129,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) radix_scatter_staged_kernel(c
 #pragma unroll
     for (int q = 0; q < kKeysPerLane; ++q) {
         const uint32_t d = digit(q);
-        const unsigned same = __match_any_sync(kFullMask, d);
+        const unsigned same = same_digit_lanes(d);
         if (d < kRadix && lane == static_cast<unsigned>(__ffs(same) - 1)) s_woff[warp][d] += __popc(same);
         __syncwarp();
     }
@@ -141,7 +155,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) radix_scatter_staged_kernel(c
 #pragma unroll
     for (int q = 0; q < kKeysPerLane; ++q) {
         const uint32_t d = digit(q);
-        const unsigned same = __match_any_sync(kFullMask, d);
+        const unsigned same = same_digit_lanes(d);
         if (d < kRadix) s_keys[s_start[d] + s_woff[warp][d] + __popc(same & below)] = key[q];
         __syncwarp();
         if (d < kRadix && lane == static_cast<unsigned>(__ffs(same) - 1)) s_woff[warp][d] += __popc(same);
