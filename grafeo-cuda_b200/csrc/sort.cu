@@ -2,9 +2,10 @@
 //
 // Each pass sorts by one 8-bit digit: per-tile digit histograms (digit-major,
 // so one exclusive scan gives every (digit, tile) its output base), then a
-// stable scatter: a tile of kSortTile keys is walked in rounds of 256 keys in
-// index order, and inside a round every key's rank among the equal digits
-// before it comes from warp matches plus a prefix over the block's warps.
+// stable scatter of each tile of kSortTile keys, staged in shared memory in
+// digit order and written out as contiguous runs (radix_scatter_staged_kernel;
+// the first form, radix_scatter_kernel, walked the tile in rounds of 256 keys
+// and wrote every key to its own address).
 // Stability makes the sort of (target << 32 | source) keys by their high word
 // keep every in-list ordered by source, so the transpose is deterministic.
 #include <algorithm>
@@ -80,13 +81,17 @@ __global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint6
 // the same order and stores them in shared memory in digit order (index order
 // inside a digit: stable); the block then writes the tile out run by run,
 // consecutive threads to consecutive addresses of a digit's output range.
+// Measured on the transpose of R-MAT 24's directed copy (505 M keys, 3
+// passes): 23.0 ms with the scatter above (each key written to its own
+// address, three block barriers per 256-key round), 18.2 ms staged.
 constexpr bool kStagedScatter = true;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSliceKeys = kSortTile / kSortWarps;
 constexpr int kKeysPerLane = kSliceKeys / 32;
 
 // Lanes of the warp holding the same digit (kRadix: a lane with no key), from
-// one ballot per digit bit (kMatchBallots) or one match instruction.
+// one ballot per digit bit (kMatchBallots) or one match instruction. The
+// ballots took the staged scatter of the same transpose from 18.2 to 15.0 ms.
 constexpr bool kMatchBallots = true;
 __device__ __forceinline__ unsigned same_digit_lanes(uint32_t d) {
     if (!kMatchBallots) return __match_any_sync(kFullMask, d);
