@@ -668,9 +668,7 @@ Error batch_run_ppr(BatchImpl& b) {
 Error batch_read_bfs(BatchImpl& b, int32_t* distances, uint32_t* reachable, int32_t* max_depth) {
     DeviceImpl& dev = *b.dev;
     const uint64_t gs = static_cast<uint64_t>(b.G) * b.S;
-    if (distances && b.keep_dist)
-        GCU_CUDA(cudaMemcpyAsync(distances, b.dist.ptr, 4ull * b.S * b.u.num_nodes, cudaMemcpyDeviceToHost, dev.stream),
-                 "copy");
+    if (distances && b.keep_dist) GCU_TRY(copy_to_host(dev, distances, b.dist.ptr, 4ull * b.S * b.u.num_nodes));
     if (reachable) GCU_CUDA(cudaMemcpyAsync(reachable, b.reachable.ptr, 4 * gs, cudaMemcpyDeviceToHost, dev.stream), "copy");
     if (max_depth) GCU_CUDA(cudaMemcpyAsync(max_depth, b.max_depth.ptr, 4 * gs, cudaMemcpyDeviceToHost, dev.stream), "copy");
     return dev.sync();
@@ -678,7 +676,7 @@ Error batch_read_bfs(BatchImpl& b, int32_t* distances, uint32_t* reachable, int3
 
 Error batch_read_ppr(BatchImpl& b, float* ranks, uint32_t* iterations, uint8_t* converged) {
     DeviceImpl& dev = *b.dev;
-    if (ranks) GCU_CUDA(cudaMemcpyAsync(ranks, b.ranks.ptr, 4ull * b.u.num_nodes, cudaMemcpyDeviceToHost, dev.stream), "copy");
+    if (ranks) GCU_TRY(copy_to_host(dev, ranks, b.ranks.ptr, 4ull * b.u.num_nodes));
     if (iterations)
         GCU_CUDA(cudaMemcpyAsync(iterations, b.iterations.ptr, 4ull * b.G, cudaMemcpyDeviceToHost, dev.stream), "copy");
     if (converged)

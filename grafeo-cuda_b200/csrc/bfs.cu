@@ -81,7 +81,7 @@ struct BfsWork {
     DeviceBuffer<uint32_t> queue[2];
     DeviceBuffer<uint32_t> degree_scan;  // V + 1
     DeviceBuffer<BfsCounters> counters;
-    BfsCounters* host_counters = nullptr;  // pinned
+    BfsCounters host_counters{};  // host copy, read after a synchronisation (plain memory)
     int symmetric = -1;                    // -1 unknown, 0 no, 1 yes
     DeviceBuffer<uint32_t> active;         // vertices with edges, ascending (symmetric graphs)
     uint32_t n_active = 0;
@@ -89,7 +89,7 @@ struct BfsWork {
     // device-driven level loop (built on first use, per schedule network)
     DeviceBuffer<BfsDevState> loop_state;
     DeviceBuffer<uint32_t> loop_scan_sums;
-    BfsDevState* host_loop_state = nullptr;  // pinned
+    BfsDevState host_loop_state{};  // host copy of the loop's final state (plain memory)
     cudaGraph_t loop_graph = nullptr;
     cudaGraphExec_t loop_exec = nullptr;
     const void* loop_net = nullptr;  // the schedule network the graph reads (NULL: fixed rule)
@@ -100,8 +100,6 @@ void destroy_bfs_work(BfsWork* w) {
     if (!w) return;
     if (w->loop_exec) cudaGraphExecDestroy(w->loop_exec);
     if (w->loop_graph) cudaGraphDestroy(w->loop_graph);
-    if (w->host_loop_state) cudaFreeHost(w->host_loop_state);
-    if (w->host_counters) cudaFreeHost(w->host_counters);
     delete w;
 }
 
@@ -688,7 +686,6 @@ static Error ensure_work(GraphImpl& g) {
     GCU_TRY(w->queue[1].allocate(dev, V));
     GCU_TRY(w->degree_scan.allocate(dev, V + 1));
     GCU_TRY(w->counters.allocate(dev, 1));
-    GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&w->host_counters), sizeof(BfsCounters)), "cudaMallocHost");
     // Bottom-up steps read in-neighbours; they equal the CSR lists only when
     // the CSR is symmetric (checked once per graph).
     bool sym = false;
@@ -795,7 +792,7 @@ Error start_run(GraphImpl& g, BfsWork& w, uint32_t source) {
 }
 
 Error read_counters(DeviceImpl& dev, BfsWork& w) {
-    GCU_CUDA(cudaMemcpyAsync(w.host_counters, w.counters.ptr, sizeof(BfsCounters), cudaMemcpyDeviceToHost, dev.stream),
+    GCU_CUDA(cudaMemcpyAsync(&w.host_counters, w.counters.ptr, sizeof(BfsCounters), cudaMemcpyDeviceToHost, dev.stream),
              "copy");
     return dev.sync();
 }
@@ -853,7 +850,6 @@ Error build_loop_graph(GraphImpl& g, BfsWork& w) {
     if (!w.loop_state.ptr) {
         GCU_TRY(w.loop_state.allocate(dev, 1));
         GCU_TRY(w.loop_scan_sums.allocate(dev, scan_device_n_tiles(V)));
-        GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&w.host_loop_state), sizeof(BfsDevState)), "cudaMallocHost");
     }
     const __nv_bfloat16* net = reinterpret_cast<const __nv_bfloat16*>(dev.schedule);
     DegreeStats stats;
@@ -989,11 +985,11 @@ Error run_loop(GraphImpl& g, BfsWork& w, uint32_t source, BfsDevState* final_sta
                w.queue[0].ptr, w.counters.ptr, w.loop_state.ptr);
     dev.launches.fetch_add(1, std::memory_order_relaxed);
     GCU_CUDA(cudaGraphLaunch(w.loop_exec, dev.stream), "cudaGraphLaunch");
-    GCU_CUDA(cudaMemcpyAsync(w.host_loop_state, w.loop_state.ptr, sizeof(BfsDevState), cudaMemcpyDeviceToHost,
+    GCU_CUDA(cudaMemcpyAsync(&w.host_loop_state, w.loop_state.ptr, sizeof(BfsDevState), cudaMemcpyDeviceToHost,
                              dev.stream),
              "copy");
     GCU_TRY(dev.sync());
-    *final_state = *w.host_loop_state;
+    *final_state = w.host_loop_state;
     return ok();
 }
 
@@ -1025,12 +1021,8 @@ Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reac
             BfsDevState fin{};
             GCU_TRY(run_loop(g, w, source, &fin));
             if (fin.failed) return kernel_error("BFS level loop stopped on an impossible state");
-            if (host_distances) {
-                GCU_CUDA(cudaMemcpyAsync(host_distances, w.dist.ptr, sizeof(int32_t) * g.num_nodes,
-                                         cudaMemcpyDeviceToHost, dev.stream),
-                         "copy distances to host");
-                GCU_TRY(dev.sync());
-            }
+            if (host_distances)
+                GCU_TRY(copy_to_host(dev, host_distances, w.dist.ptr, sizeof(int32_t) * g.num_nodes));
             *reachable = fin.reached;
             *max_depth = fin.level;
             return ok();
@@ -1043,11 +1035,11 @@ Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reac
                    static_cast<unsigned long long>(g.num_edges), 0u, 0, 0, valid, g.num_nodes, nullptr);
     GCU_TRY(read_counters(dev, w));
     BfsState st;
-    advance(st, *w.host_counters, true, 0, g.num_edges);
+    advance(st, w.host_counters, true, 0, g.num_edges);
     while (st.frontier_q > 0) {
         int variant = fixed_rule(st, sym, g.num_nodes);
         if (net) {
-            const int c = w.host_counters->choice;
+            const int c = w.host_counters.choice;
             if (c >= 0 && ((valid >> c) & 1u)) variant = c;
         }
         GCU_TRY(launch_step(g, w, variant, st));
@@ -1056,15 +1048,10 @@ Error bfs(GraphImpl& g, uint32_t source, int32_t* host_distances, uint32_t* reac
                        static_cast<unsigned long long>(st.unexplored), st.reached, st.level + 1,
                        variant == kPull ? 1 : 0, valid, g.num_nodes, nullptr);
         GCU_TRY(read_counters(dev, w));
-        if (w.host_counters->discovered == 0) break;
-        advance(st, *w.host_counters, false, variant, g.num_edges);
+        if (w.host_counters.discovered == 0) break;
+        advance(st, w.host_counters, false, variant, g.num_edges);
     }
-    if (host_distances) {
-        GCU_CUDA(cudaMemcpyAsync(host_distances, w.dist.ptr, sizeof(int32_t) * g.num_nodes, cudaMemcpyDeviceToHost,
-                                 dev.stream),
-                 "copy distances to host");
-        GCU_TRY(dev.sync());
-    }
+    if (host_distances) GCU_TRY(copy_to_host(dev, host_distances, w.dist.ptr, sizeof(int32_t) * g.num_nodes));
     *reachable = st.reached;
     *max_depth = st.level;
     return ok();
@@ -1108,7 +1095,7 @@ Error bfs_trace(GraphImpl& g, uint32_t source, uint64_t explore_seed, std::vecto
                static_cast<unsigned long long>(g.num_edges), 0u, 0, 0, valid, g.num_nodes, feats.ptr);
     GCU_TRY(read_counters(dev, w));
     BfsState st;
-    advance(st, *w.host_counters, true, 0, g.num_edges);
+    advance(st, w.host_counters, true, 0, g.num_edges);
     std::vector<float> host_feats(kSchedIn);
     GCU_CUDA(cudaMemcpy(host_feats.data(), feats.ptr, 4 * kSchedIn, cudaMemcpyDeviceToHost), "copy");
     while (st.frontier_q > 0) {
@@ -1157,7 +1144,7 @@ Error bfs_trace(GraphImpl& g, uint32_t source, uint64_t explore_seed, std::vecto
         GCU_CUDA(cudaMemcpyAsync(host_feats.data(), feats.ptr, 4 * kSchedIn, cudaMemcpyDeviceToHost, dev.stream),
                  "copy");
         GCU_TRY(read_counters(dev, w));
-        const BfsCounters c = *w.host_counters;
+        const BfsCounters c = w.host_counters;
         for (int v = 0; v < kSchedOut; ++v) {
             rec.times_us[v] = __builtin_nanf("");
             if (!((valid >> v) & 1u)) continue;

