@@ -244,6 +244,7 @@ __global__ void __launch_bounds__(kSortThreads, kScatterMinCtas) radix_scatter_s
 constexpr bool kKeysInSmem = true;
 constexpr bool kPrefetchNextTile = true;
 constexpr size_t kSmemScatterBytes = 2 * sizeof(uint64_t) * kSortTile;
+static_assert(!kKeysInSmem || kKeysPerLane % 2 == 0, "two keys' rank words per register");
 
 __global__ void __launch_bounds__(kSortThreads, kScatterMinCtas) radix_scatter_smem_kernel(
     const uint64_t* __restrict__ in, uint64_t* __restrict__ out, uint64_t n, uint32_t shift, uint32_t nctas,
